@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""Benchmark of the TSUNER hot path on B200: cell-steps/s of the time step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload nwave4096|hump512|humps8192] [--no-cpu-baseline]
+
+One "step" is one full time step of the scheme (2 RK stages: MUSCL faces,
+edge fluxes with bedload, volume update, running extrema, CFL dt) over the
+whole grid.  Default workload: the 4096^2 shelf with the west N-wave
+(seeded synthetic inputs, no dataset).  The state (671 MB in FP64) is far
+larger than the 126 MB L2, so no L2 flush is needed between steps.
+
+--impl ours       the product library (libtsuner_b200.so) through its C ABI
+--impl reference  the reference's own CUDA kernels, unmodified, built by
+                  oracle/build_ref.py and driven step by step on the same GPU
+                  and inputs (the reference has no CPU implementation of the
+                  path); without a GPU or without oracle/_ref it falls back to
+                  the oracle port on the host cores.
+
+Multi-GPU (torchrun, one rank per GPU): every rank advances its own replica
+(weak scaling, no data-path collective); the reported time is the max over
+ranks of the device-timed region.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s: FP32 fused vs FP64 plain at stated L-inf error; % HBM peak"
+# algorithmic DRAM bytes per cell-step of the fused FP64 form, 5 state planes:
+# stage 1 reads U^n, writes U*; stage 2 reads U* and U^n, writes U^{n+1}
+# (5 x 5 planes x 8 B), mask read twice (2 x 1 B), hmax/bmin/eta_max RMW (48 B)
+BYTES_PER_CELL_STEP = {"f64": 5 * 5 * 8 + 2 + 3 * 16}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload(name):
+    from tsuner_b200 import workloads as W
+    if name == "nwave4096":
+        return W.nwave_shelf(4096, 4096, 5.0), "nwave_shelf 4096x4096 dx=5m (fractal k^-3 shelf, 20% dry, mask, west N-wave 3m/600s, SLR+0.5m)"
+    if name == "nwave2048":
+        return W.nwave_shelf(2048, 2048, 10.0), "nwave_shelf 2048x2048 dx=10m (profiling case: 168 MB FP64 state > L2)"
+    if name == "hump512":
+        return W.hump(512, 512, 10.0), "hump 512x512 dx=10m (2m Gaussian hump, noisy 2% slope, walls)"
+    if name == "humps8192":
+        return W.humps_shelf(8192, 8192, 5.0), "humps_shelf 8192x8192 dx=5m (8 seeded humps, walls)"
+    raise SystemExit("unknown workload " + name)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.f = tempfile.TemporaryFile(mode="w+")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc:
+            return None
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f:
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                mx.append(float(c[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def dist_setup(n):
+    if n <= 1 or "RANK" not in os.environ:
+        return 0, 1, int(os.environ.get("LOCAL_RANK", 0)), None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist.get_rank(), dist.get_world_size(), local, dist
+
+
+def dist_max(dist, v, local):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda:%d" % local)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, local):
+    if dist is not None:
+        import torch
+        dist.barrier(device_ids=[local])
+        torch.cuda.synchronize(local)
+
+
+def cpu_baseline(max_seconds=20.0):
+    """The oracle port (OpenMP C) on this host's cores, on a bounded sample of
+    the same workload generator (4096 x 512 strip of the shelf)."""
+    import oracle
+    from tsuner_b200 import workloads as W
+    w = W.nwave_shelf(4096, 512, 5.0)
+    r = oracle.OracleRun(w.p, w.sw, w.V, w.mask, w.CC, w.tCC)
+    r.run(1)  # first touch of the work arrays
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        r.run(1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > max_seconds or steps >= 200:
+            break
+    return {"value": w.ncells * steps / el / 1e6, "unit": "Mcell-steps/s", "cores": oracle.max_threads(),
+            "kind": "port", "sample": "nwave_shelf 4096x512 strip, %d steps (%.1f s) on %d threads"
+            % (steps, el, oracle.max_threads())}
+
+
+def traffic_from_profiles(name):
+    """Per-launch DRAM bytes of the stage kernels recorded by ncu (profiles/)."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    try:
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 3 and parts[0] == name:
+                return float(parts[1]), float(parts[2])  # bytes per cell-step, cells of the capture
+    except OSError:
+        pass
+    return None
+
+
+def run_ours(a, rank, world, local, dist):
+    import tsuner_b200 as T
+    w, desc = workload(a.workload)
+    n = w.ncells
+    s = T.Solver(w.p, w.sw, device=local)
+    # ---- device-timed region (inputs resident in HBM)
+    s.set_state(w.V)
+    s.set_mask(w.mask)
+    if w.sw.read_files:
+        s.set_boundary_series(w.CC, w.tCC)
+    s.reset()
+    s.step(a.warmup)
+    s.sync()
+    barrier(dist, local)
+    with Clocks(local) as clk:
+        s.step(a.steps)
+        s.sync()
+    ms = s.last_ms()
+    launches = s.last_launches()
+    ms_max = dist_max(dist, ms, local)
+    # ---- end to end through the C ABI with host buffers
+    barrier(dist, local)
+    t0 = time.perf_counter()
+    s.set_state(w.V)
+    s.set_mask(w.mask)
+    if w.sw.read_files:
+        s.set_boundary_series(w.CC, w.tCC)
+    s.reset()
+    s.step(a.steps)
+    Vout = s.state()
+    ext = s.extrema()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = dist_max(dist, e2e_s, local)
+    s.close()
+    assert np.isfinite(Vout).all()
+    h2d = 5 * 8 * n + 4 * n + (w.CC.nbytes + w.tCC.nbytes if w.sw.read_files else 0)
+    d2h = 5 * 8 * n + 3 * 8 * n
+    if rank != 0:
+        return None
+    value = world * n * a.steps / (ms_max / 1e3) / 1e6
+    hbm, kind = peaks()
+    bpc = BYTES_PER_CELL_STEP["f64"]
+    achieved = bpc * n * a.steps / (ms / 1e3) / 1e9
+    tr = traffic_from_profiles("stage64_" + a.workload)
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mcell-steps/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generators, no dataset)",
+        "config": {"workload": desc, "form": "fp64 plain (one fused kernel per RK stage)",
+                   "cells": n, "l2": "state %.0f MB > 126 MB L2, no flush needed" % (5 * 8 * n / 1e6),
+                   "parallelism": "replicas x%d" % world},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "peak_kind": kind,
+                     "bytes_per_cell_step": bpc,
+                     "traffic": None if tr is None else round(tr[0] * n / 2.0, 0),
+                     "note": "FP64 plain form is FP64-pipe bound; algorithmic bytes over device time"},
+        "gpu_launches": launches,
+        "e2e": {"value": round(world * n * a.steps / e2e_s / 1e6, 3), "unit": "Mcell-steps/s",
+                "h2d_bytes_per_step": int(h2d / a.steps), "d2h_bytes_per_step": int(d2h / a.steps),
+                "what": "tsu_set_state/mask/series + tsu_reset + tsu_step(K) + tsu_get_state/extrema, host buffers"},
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline()
+    return line
+
+
+def run_reference(a, rank, world, local, dist):
+    if rank != 0:
+        return None
+    import oracle
+    w, desc = workload(a.workload)
+    n = w.ncells
+    gpu_ok = False
+    try:
+        import tsuner_b200 as T
+        gpu_ok = T.lib().checkCUDAsupport(local) == 0
+    except Exception:
+        gpu_ok = False
+    if gpu_ok and oracle.ref_available("default"):
+        CC, tCC = (w.CC, w.tCC) if w.sw.read_files else oracle_expired(w)
+        oracle.ref_run("default", w.p, w.V, w.mask, CC, tCC, a.warmup, device=local)
+        with Clocks(local) as clk:
+            t0 = time.perf_counter()
+            r = oracle.ref_run("default", w.p, w.V, w.mask, CC, tCC, a.steps, device=local)
+            wall = time.perf_counter() - t0
+        value = n * a.steps / (r["ms"] / 1e3) / 1e6
+        return {"metric": METRIC, "value": round(value, 3), "unit": "Mcell-steps/s", "n_gpus": 1,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(r["ms"] / a.steps, 4),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generators, no dataset)", "impl": "reference",
+                "reference_kind": "reference CUDA build (unmodified GPU/*.cu kernels, -O2 -fmad=false -rdc -dlto, sm_100a)",
+                "config": {"workload": desc, "cells": n, "parallelism": "single GPU"},
+                "e2e": {"value": round(n * a.steps / wall / 1e6, 3), "unit": "Mcell-steps/s",
+                        "h2d_bytes_per_step": int((5 * 8 * n + 4 * n) / a.steps),
+                        "d2h_bytes_per_step": int((5 * 8 * n + 3 * 8 * n) / a.steps),
+                        "what": "whole harness call: allocation, upload, K steps, download"},
+                "clocks": clk.summary()}
+    cb = cpu_baseline()
+    return {"metric": METRIC, "value": cb["value"], "unit": "Mcell-steps/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference", "config": {"workload": desc},
+            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "Mcell-steps/s",
+                                        "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def oracle_expired(w):
+    from tsuner_b200 import workloads as W
+    return W.expired_series(w.p.npx, w.p.npy)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="nwave4096")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+    rank, world, local, dist = dist_setup(a.gpus)
+    try:
+        if a.impl == "reference":
+            line = run_reference(a, rank, world, local, dist)
+        else:
+            line = run_ours(a, rank, world, local, dist)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

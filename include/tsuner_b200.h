@@ -1,0 +1,199 @@
+/*
+ * tsuner_b200.h -- C ABI of the B200-native TSUNER hot path.
+ *
+ * Two layers:
+ *  1. Drop-in entry points with the reference signatures and return codes:
+ *       TSUNER()            replaces TSUNER.h:39 / GPU/main_TSUNER.cu:21
+ *       checkCUDAsupport()  replaces TSUNER.h:41 / GPU/CheckCUDASupport.cu:21
+ *       initializeGPU()     replaces TSUNER.h:42 / GPU/InitializeGPU.cu:23
+ *  2. Fine-grained tsu_* calls (no counterpart in the reference, whose only
+ *     interface is the whole-run TSUNER()): create a solver, upload a state,
+ *     step it a given number of times, read the state and extrema back.
+ *     Tests, bench.py and the ensemble runner use these.
+ *
+ * All pointers are plain host pointers unless a name says `device`.
+ * All calls return an int status (TSU_OK == 0) unless stated otherwise.
+ * Nothing here takes or returns framework (torch) types.
+ */
+#ifndef TSUNER_B200_H
+#define TSUNER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__CUDACC__) || defined(__VECTOR_TYPES_H__)
+#include <vector_types.h>
+typedef double2 tsu_double2;
+#else
+/* Same size and alignment as CUDA's double2 (vector_types.h). */
+typedef struct tsu_double2 { double x, y; } __attribute__((aligned(16))) tsu_double2;
+#endif
+
+#ifndef TSU_NO_SIMPARAMS
+/* Layout-identical to `struct SimParams` of TSUNER.h:10-30 (passed by value
+ * to TSUNER()).  Units: metres, seconds.  FR is the Chezy coefficient already
+ * divided by 8 (Problem_loader.cxx:337-339); Q, Opar, HQB are the derived
+ * values of Problem_loader.cxx:340-342. */
+typedef struct SimParams {
+    double xmin;
+    double xmax;
+    double ymin;
+    double ymax;
+    double total_time, save_time;
+    int npx, npy, nvol;
+    double CFL;
+    double Q, R;
+    double porosity;
+    double DS;
+    double FR;
+    double Opar;
+    double OC;
+    double Dsg;
+    double HQB;
+    double vmax;
+    double epsilon_h;
+    double dx;
+    double dy;
+} SimParams;
+#endif
+
+/* Status codes.  1 and 2 keep the meaning of the reference TSUNER() return
+ * values (GPU/main_TSUNER.cu:20, main_TSUNER.cxx:91-98). */
+enum {
+    TSU_OK = 0,
+    TSU_ERR_GPU_OOM = 1,
+    TSU_ERR_HOST_OOM = 2,
+    TSU_ERR_INVALID = 3,      /* bad argument / unsupported size or switch */
+    TSU_ERR_CUDA = 4,         /* a CUDA runtime call failed */
+    TSU_ERR_NO_DEVICE = 5,    /* no usable CUDA device / bad index */
+    TSU_ERR_NONFINITE = 6,    /* the device detected a NaN/Inf state */
+    TSU_ERR_IO = 7            /* output file could not be written */
+};
+
+/* Run-time form of the reference's compile-time switches
+ * (Sim_parameters.hxx:45-54).  tsu_switches_default() fills the values the
+ * reference ships with. */
+typedef struct TsuSwitches {
+    int order;        /* 1 | 2                                   (`order`)   */
+    int rk;           /* 1 = Runge-Kutta (only 1 is implemented) (`RK`)      */
+    int wbc;          /* 0 free | 1 wall | 2 periodic            (`WBC`)     */
+    int bedload;      /* 0 | 1                                   (`BEDLOAD`) */
+    int suspension;   /* 0 | 1                                   (`SUSPENSION`) */
+    int read_files;   /* 1: boundary edges follow the CC series while
+                         t < tCC[timeCC-2], then act as walls  (`Read_files`) */
+    int bedload_law;  /* 0 = reference Ashida-Michiue law (GPU/SedFlux.cuh:150-168);
+                         1 = Grass law q_b = A_g u |u|^2 / (1-p) (no reference
+                         counterpart) */
+    int precision;    /* 0 = FP64 plain form (bitwise with the reference);
+                         1 = FP32 precision form                              */
+    double grass_ag;  /* A_g of the Grass law                               */
+} TsuSwitches;
+
+/* Per-run constants of the sediment laws, hoisted out of the per-cell code.
+ * Each is the exact expression the reference evaluates per cell
+ * (GPU/Reconstructor.cu:64-77, GPU/SedFlux.cuh:51-99,150-168), evaluated
+ * once on the device so the device pow() is used. */
+typedef struct TsuConsts {
+    double vs;        /* settling velocity                                  */
+    double Rp;        /* particle Reynolds number                           */
+    double A_er;      /* alpha1 * pow(Rp, alpha2)                           */
+    double sqrt_FR;   /* sqrt(FR)                                           */
+    double VP;        /* vs * (1 - porosity)                                */
+    double K_dep;     /* 1.64 + 0.4 * pow(DS/Dsg, 1.64)                     */
+    double sqrt_OC;   /* sqrt(OC)                                           */
+    double DS5;       /* 5 * DS                                             */
+} TsuConsts;
+
+typedef struct TsuSolver TsuSolver;
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- drop-in entry points ---------------- */
+
+/* Whole run, as the reference: uploads the state (h, (qx,qy), H; hc = 0),
+ * steps while t < params.total_time, writes <input_prefix>.nc with the
+ * reference layout (GPU/netcdf.cu:38-435) and the wall time into *tiempo.
+ * d, dyrup, time_dyrup, tides_bd, tides_time, tidesNPT are accepted and
+ * ignored, as in the reference build (SPL == 0, tides commented out).
+ * The switches are the process-wide defaults (tsu_set_default_switches). */
+#ifdef __cplusplus
+int TSUNER(double *dVh, tsu_double2 *dVhu, double *dVH, int *fixH, SimParams params,
+           char *input_prefix, double *d, double *CC, double *tCC, unsigned long timeCC,
+           double *dyrup, float *time_dyrup, double &tiempo, int CudaDevice,
+           double *tides_bd, float *tides_time, int tidesNPT);
+#else
+int TSUNER(double *dVh, tsu_double2 *dVhu, double *dVH, int *fixH, SimParams params,
+           char *input_prefix, double *d, double *CC, double *tCC, unsigned long timeCC,
+           double *dyrup, float *time_dyrup, double *tiempo, int CudaDevice,
+           double *tides_bd, float *tides_time, int tidesNPT);
+#endif
+/* 0 ok, 1 no GPU, 2 no CUDA-capable GPU, 3 bad device index. */
+int checkCUDAsupport(int cudaDevice);
+/* Creates the CUDA context on the current device (warm-up). */
+void initializeGPU(void);
+
+/* ---------------- configuration ---------------- */
+
+int tsu_switches_default(TsuSwitches *sw);
+int tsu_set_default_switches(const TsuSwitches *sw);   /* used by TSUNER() */
+int tsu_get_default_switches(TsuSwitches *sw);
+/* Derived parameters of Problem_loader.cxx:337-342 from the data.dat values
+ * (FR given as in data.dat, i.e. before the /8). */
+int tsu_derive_params(SimParams *p, double friction_datdat);
+/* Parses a reference data.dat (Problem_loader.cxx:264-342 format).  Fills
+ * p (xmin..Dsg, derived Q/Opar/HQB, nvol; dx/dy from the box), the output
+ * prefix, the three input file names, SLR and the tides file name.  Strings
+ * are written NUL-terminated into buffers of `cap` bytes. */
+int tsu_parse_data_dat(const char *path, SimParams *p, char *prefix, char *bathy_file,
+                       char *ic_file, char *mask_file, double *slr, char *tides_file,
+                       size_t cap);
+
+/* ---------------- solver ---------------- */
+
+int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches *sw, int device);
+int tsu_destroy(TsuSolver *s);
+/* Host planes of nvol doubles each, row-major [npy][npx]; hc may be NULL (0). */
+int tsu_set_state(TsuSolver *s, const double *h, const double *qx, const double *qy,
+                  const double *H, const double *hc);
+/* Binary mask (1 = erodible, 0 = fixed), nvol ints, values must be 0 or 1.
+ * NULL = all erodible. */
+int tsu_set_mask(TsuSolver *s, const int *fixH);
+/* Boundary series CC[timeCC][2npx+2npy][4] (eta, u, v, H) and its uniform
+ * time axis tCC[timeCC] (interpolations.cxx:368-774 layout). */
+int tsu_set_boundary_series(TsuSolver *s, const double *CC, const double *tCC,
+                            unsigned long timeCC);
+/* Resets t = 0, the running extrema to -1e30 and computes the initial dt
+ * (GPU/main_TSUNER.cu:142-149).  Must follow tsu_set_state. */
+int tsu_reset(TsuSolver *s);
+/* Enqueues nsteps time steps on the solver's stream (no host sync). */
+int tsu_step(TsuSolver *s, long nsteps);
+/* Steps while t < t_end (the reference loop condition), at most max_steps;
+ * *steps_done gets the number of steps taken.  Synchronises. */
+int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *steps_done);
+int tsu_sync(TsuSolver *s);
+/* 5*nvol doubles SoA (h, qx, qy, H, hc). */
+int tsu_get_state(TsuSolver *s, double *V);
+int tsu_get_extrema(TsuSolver *s, double *hmax, double *bmin_rawH, double *eta_max);
+int tsu_get_time(TsuSolver *s, double *t, double *dt, long *steps);
+int tsu_get_consts(TsuSolver *s, TsuConsts *k);
+/* Device timing of the last tsu_step() call in ms (CUDA events). */
+int tsu_last_step_ms(TsuSolver *s, double *ms);
+/* Number of kernel launches the last tsu_step() issued. */
+int tsu_last_step_launches(TsuSolver *s, long *launches);
+/* Device pointer of the current state (plane-major, row pitch in elements). */
+int tsu_state_device(TsuSolver *s, void **ptr, long *pitch_elems, long *plane_elems,
+                     int *elem_bytes);
+const char *tsu_strerror(int code);
+/* Detail text of the last failing call on this thread ("" if none). */
+const char *tsu_last_error(void);
+const char *tsu_version(void);
+/* sizeof(SimParams), sizeof(TsuSwitches), sizeof(TsuConsts) as compiled
+ * into the library, for binding checks (host only, no device use). */
+int tsu_struct_sizes(size_t out[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TSUNER_B200_H */

@@ -1,0 +1,149 @@
+"""Python bindings of the CPU oracle and of the reference checker builds.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py -- never by the product package.
+
+  liboracle.so            plain-C restatement of the reference step (oracle.c)
+  _ref/<v>/libtsuner_ref.so  the reference's own CUDA kernels, unmodified, built
+                          per switch variant by build_ref.py and driven by
+                          ref_build/ref_harness.cu (needs a GPU)
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from tsuner_b200.abi import SimParams, TsuConsts, TsuSwitches
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = {}
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def build():
+    import subprocess
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        L.orc_consts.argtypes = [C.POINTER(SimParams), C.POINTER(TsuConsts)]
+        L.orc_consts.restype = None
+        L.orc_initial_dt.argtypes = [C.POINTER(SimParams), C.POINTER(TsuSwitches), _dp, C.c_int]
+        L.orc_initial_dt.restype = C.c_double
+        L.orc_run.argtypes = [C.POINTER(SimParams), C.POINTER(TsuSwitches), C.c_void_p, _dp, _ip,
+                              C.c_void_p, C.c_void_p, C.c_ulong, C.c_void_p, C.c_void_p, C.c_void_p,
+                              C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_long, C.c_double, C.c_int]
+        L.orc_run.restype = C.c_long
+        L.orc_init_extrema.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_max_threads.restype = C.c_int
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def consts(p):
+    k = TsuConsts()
+    lib().orc_consts(C.byref(p), C.byref(k))
+    return k
+
+
+def max_threads():
+    return lib().orc_max_threads()
+
+
+def initial_dt(p, sw, V, nthreads=0):
+    return lib().orc_initial_dt(C.byref(p), C.byref(sw), np.ascontiguousarray(V, np.float64), nthreads)
+
+
+class OracleRun:
+    """Host state for the oracle: V (5, npy, npx) SoA, extrema, t, dt."""
+
+    def __init__(self, p, sw, V, mask=None, CC=None, tCC=None, kconsts=None, nthreads=0):
+        self.p, self.sw = p, sw
+        n = p.npx * p.npy
+        self.V = np.ascontiguousarray(V, np.float64).reshape(5, p.npy, p.npx).copy()
+        self.mask = (np.ones(n, np.int32) if mask is None
+                     else np.ascontiguousarray(mask, np.int32).reshape(-1).copy())
+        self.CC = None if CC is None else np.ascontiguousarray(CC, np.float64)
+        self.tCC = None if tCC is None else np.ascontiguousarray(tCC, np.float64)
+        self.timeCC = 0 if tCC is None else len(self.tCC)
+        self.k = kconsts
+        self.nthreads = nthreads
+        self.hmax = np.empty(n)
+        self.bmin = np.empty(n)
+        self.eta_max = np.empty(n)
+        lib().orc_init_extrema(n, _ptr(self.hmax), _ptr(self.bmin), _ptr(self.eta_max))
+        self.t = C.c_double(0.0)
+        self.dt = C.c_double(-1.0)
+        self.steps = 0
+
+    def run(self, nsteps=-1, t_end=0.0):
+        k = None if self.k is None else C.byref(self.k)
+        n = lib().orc_run(C.byref(self.p), C.byref(self.sw), k, self.V.reshape(-1), self.mask,
+                          _ptr(self.CC), _ptr(self.tCC), self.timeCC, _ptr(self.hmax),
+                          _ptr(self.bmin), _ptr(self.eta_max), C.byref(self.t), C.byref(self.dt),
+                          nsteps, t_end, self.nthreads)
+        if n < 0:
+            raise RuntimeError("oracle run failed (%d)" % n)
+        self.steps += n
+        return n
+
+
+# ---------------------------------------------------------------- reference
+def ref_path(variant="default"):
+    return os.path.join(HERE, "_ref", variant, "libtsuner_ref.so")
+
+
+def ref_available(variant="default"):
+    return os.path.exists(ref_path(variant))
+
+
+def ref_lib(variant="default"):
+    if variant not in _REF:
+        L = C.CDLL(ref_path(variant))
+        L.ref_run.argtypes = [SimParams, _dp, _ip, C.c_void_p, C.c_void_p, C.c_ulong, C.c_long,
+                              C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+                              C.POINTER(C.c_double), C.POINTER(C.c_long), C.POINTER(C.c_double), C.c_int]
+        L.ref_run.restype = C.c_int
+        L.ref_switches.argtypes = [_ip]
+        L.ref_initial_dt.argtypes = [SimParams, _dp, C.POINTER(C.c_double), C.c_int]
+        _REF[variant] = L
+    return _REF[variant]
+
+
+def ref_switches(variant="default"):
+    out = np.zeros(6, np.int32)
+    ref_lib(variant).ref_switches(out)
+    return dict(zip(("order", "rk", "wbc", "bedload", "suspension", "read_files"), out.tolist()))
+
+
+def ref_run(variant, p, V, mask=None, CC=None, tCC=None, nsteps=1, device=0):
+    """Runs the reference build for nsteps; returns dict with V, extrema, t, dt, ms."""
+    n = p.npx * p.npy
+    Vh = np.ascontiguousarray(V, np.float64).reshape(-1).copy()
+    m = np.ones(n, np.int32) if mask is None else np.ascontiguousarray(mask, np.int32).reshape(-1)
+    hmax, bmin, eta = np.empty(n), np.empty(n), np.empty(n)
+    t, dt, ms = C.c_double(), C.c_double(), C.c_double()
+    steps = C.c_long()
+    CCa = None if CC is None else np.ascontiguousarray(CC, np.float64)
+    tCa = None if tCC is None else np.ascontiguousarray(tCC, np.float64)
+    rc = ref_lib(variant).ref_run(p, Vh, m, _ptr(CCa), _ptr(tCa), 0 if tCa is None else len(tCa),
+                                  nsteps, _ptr(hmax), _ptr(bmin), _ptr(eta), C.byref(t),
+                                  C.byref(dt), C.byref(steps), C.byref(ms), device)
+    if rc != 0:
+        raise RuntimeError("reference harness failed (%d)" % rc)
+    return dict(V=Vh.reshape(5, p.npy, p.npx), hmax=hmax.reshape(p.npy, p.npx),
+                bmin=bmin.reshape(p.npy, p.npx), eta_max=eta.reshape(p.npy, p.npx),
+                t=t.value, dt=dt.value, ms=ms.value, steps=steps.value)

@@ -1,0 +1,115 @@
+"""Build recipe for the reference checker (oracle/_ref/).
+
+TEST INFRASTRUCTURE ONLY.  Compiles the reference TSUNER CUDA sources,
+unmodified, where they lie under the reference checkout, together with
+oracle/ref_build/ref_harness.cu into one shared library per compile-time
+switch variant:  oracle/_ref/<variant>/libtsuner_ref.so
+
+The reference selects its scheme with #defines in Sim_parameters.hxx
+(order, RK, WBC, BEDLOAD, SUSPENSION, Read_files; Sim_parameters.hxx:45-54).
+A variant is built without copying or editing any reference file: a small
+generated header is force-included (-include) that first includes the
+reference Sim_parameters.hxx (which is `#pragma once`) and then re-#defines
+the switches, so the later `#include "Sim_parameters.hxx"` of TSUNER.h is a
+no-op and the kernels see the variant's values.
+
+Flags follow GPU/makefile:10 (-O2 -fmad=false -rdc=true -dlto) with
+-arch=native replaced by sm_100a (this container has no GPU to query).
+
+Usage:  python oracle/build_ref.py [--ref PATH] [variant ...]
+The built .so files travel to the GPU box; the reference tree is only read
+here, at build time.
+"""
+import argparse
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+DEFAULT_REF = "/root/reference"
+
+# name -> switch overrides (unset keys keep the reference defaults:
+# order 2, RK 1, WBC 1, BEDLOAD 1, SUSPENSION 1, Read_files 1)
+VARIANTS = {
+    "default": {},
+    "rf0_wbc1": {"Read_files": 0, "WBC": 1},
+    "rf0_wbc0": {"Read_files": 0, "WBC": 0},
+    "rf0_wbc2": {"Read_files": 0, "WBC": 2},
+    "order1": {"order": 1},
+    "nosed": {"BEDLOAD": 0, "SUSPENSION": 0},
+}
+
+KERNEL_SOURCES = [
+    "GPU/Reconstructor.cu",
+    "GPU/VolumeSolver.cu",
+    "GPU/Volume_kernel.cu",
+    "GPU/Reduction_kernel_min.cu",
+]
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = ["-O2", "-arch=sm_100a", "-fmad=false", "-rdc=true", "-dlto",
+         "-Xcompiler", "-fPIC", "-w"]
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError("reference build step failed")
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
+
+
+def build_variant(name, ref=DEFAULT_REF, force=False):
+    sw = VARIANTS[name]
+    vdir = os.path.join(OUT, name)
+    os.makedirs(vdir, exist_ok=True)
+    so = os.path.join(vdir, "libtsuner_ref.so")
+    srcs = [os.path.join(ref, s) for s in KERNEL_SOURCES]
+    deps = srcs + [os.path.join(HERE, "ref_build", "ref_harness.cu"), __file__,
+                   os.path.join(ref, "Sim_parameters.hxx"), os.path.join(ref, "GPU", "SedFlux.cuh")]
+    if not force and _newer(so, deps):
+        return so
+    ov = os.path.join(vdir, "switches.h")
+    with open(ov, "w") as f:
+        f.write("/* generated by oracle/build_ref.py: variant %s */\n" % name)
+        f.write('#include "%s"\n' % os.path.join(ref, "Sim_parameters.hxx"))
+        for k, v in sw.items():
+            f.write("#undef %s\n#define %s %d\n" % (k, k, v))
+    inc = ["-include", ov, "-I" + os.path.join(ref, "GPU"), "-I" + ref,
+           "-I" + os.path.join(HERE, "ref_build")]
+    objs = []
+    for s in srcs + [os.path.join(HERE, "ref_build", "ref_harness.cu")]:
+        o = os.path.join(vdir, os.path.basename(s).replace(".cu", ".o"))
+        _run([NVCC] + FLAGS + inc + ["-c", s, "-o", o])
+        objs.append(o)
+    dl = os.path.join(vdir, "dlink.o")
+    _run([NVCC, "-arch=sm_100a", "-dlto", "-Xcompiler", "-fPIC", "-dlink"] + objs + ["-o", dl])
+    _run(["g++", "-shared", "-o", so] + objs + [dl, "-L/usr/local/cuda/lib64", "-lcudart"])
+    for o in objs + [dl]:
+        os.remove(o)
+    return so
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default=DEFAULT_REF)
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("variants", nargs="*")
+    a = ap.parse_args(argv)
+    if not os.path.isdir(a.ref):
+        print("reference tree not present; keeping prebuilt oracle/_ref")
+        return 0
+    for v in (a.variants or list(VARIANTS)):
+        print(build_variant(v, a.ref, a.force))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

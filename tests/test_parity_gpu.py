@@ -1,0 +1,215 @@
+"""GPU parity: the fused sm_100a kernels (through the C ABI) against
+  (a) the CPU oracle on small seeded cases, for every switch combination, and
+  (b) the reference's own CUDA build (oracle/_ref, its unmodified kernels
+      driven step by step) on the same inputs, up to the full 512^2 x 2000
+      step configuration and a 4096^2 slice of the shelf configuration.
+
+The bar (stated per field after the run): max|new - ref| / max|ref| <= 1e-12,
+wet/dry flags (h > epsilon_h) identical, and the same number of steps and
+simulated time.  Because the FP64 form keeps the reference's operation order
+and is built with -fmad=false like the reference, the tests also assert that
+the fields are equal value for value (0 == -0).
+"""
+import numpy as np
+import pytest
+
+import oracle
+import tsuner_b200 as T
+from tsuner_b200 import workloads as W
+from tsuner_b200.abi import make_switches
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("h", "qx", "qy", "H", "hc")
+REL_TOL = 1e-12
+
+
+def run_product(w, nsteps, sw=None):
+    sw = sw or w.sw
+    s = T.Solver(w.p, sw)
+    s.set_state(w.V)
+    s.set_mask(w.mask)
+    if sw.read_files:
+        s.set_boundary_series(w.CC, w.tCC)
+    s.reset()
+    s.step(nsteps)
+    out = dict(V=s.state())
+    out["hmax"], out["bmin"], out["eta_max"] = s.extrema()
+    out["t"], out["dt"], out["steps"] = s.time()
+    out["k"] = s.consts()
+    s.close()
+    return out
+
+
+def run_oracle(w, nsteps, k, sw=None):
+    sw = sw or w.sw
+    r = oracle.OracleRun(w.p, sw, w.V, w.mask, w.CC if sw.read_files else None,
+                         w.tCC if sw.read_files else None, kconsts=k)
+    r.run(nsteps)
+    shp = (w.p.npy, w.p.npx)
+    return dict(V=r.V, hmax=r.hmax.reshape(shp), bmin=r.bmin.reshape(shp), eta_max=r.eta_max.reshape(shp),
+                t=r.t.value, dt=r.dt.value, steps=r.steps)
+
+
+def rel_err(a, b):
+    scale = max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max() / scale
+
+
+def assert_parity(new, ref, eps_h, exact=True, extrema=True):
+    for f, name in enumerate(FIELDS):
+        e = rel_err(new["V"][f], ref["V"][f])
+        assert e <= REL_TOL, "%s rel err %.3e" % (name, e)
+        if exact:
+            assert np.array_equal(new["V"][f], ref["V"][f]), "%s not value-identical (rel %.3e)" % (name, e)
+    assert np.array_equal(new["V"][0] > eps_h, ref["V"][0] > eps_h)
+    if extrema:
+        for k in ("hmax", "bmin", "eta_max"):
+            assert rel_err(new[k], ref[k]) <= REL_TOL, k
+            if exact:
+                assert np.array_equal(new[k], ref[k]), k
+    assert new["t"] == ref["t"] and new["dt"] == ref["dt"]
+
+
+# ------------------------------------------------------------- vs the oracle
+CASES = {
+    "walls_o2": dict(order=2, wbc=1),
+    "walls_o1": dict(order=1, wbc=1),
+    "free_o2": dict(order=2, wbc=0),
+    "periodic_o2": dict(order=2, wbc=2),
+    "no_sediment": dict(order=2, wbc=1, bedload=0, suspension=0),
+    "grass_law": dict(order=2, wbc=1, bedload_law=1, grass_ag=1e-3),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_hump_vs_oracle(case):
+    w = W.hump(61, 45, 10.0, sigma=90.0)
+    w.mask = W.harbour_mask(61, 45, np.random.default_rng(7))
+    sw = make_switches(read_files=0, **CASES[case])
+    new = run_product(w, 120, sw)
+    ref = run_oracle(w, 120, new["k"], sw)
+    assert ref["steps"] == 120 and new["steps"] == 120
+    assert_parity(new, ref, w.p.epsilon_h)
+
+
+@pytest.mark.parametrize("shape", [(1, 50), (50, 1), (3, 3), (33, 9), (8, 40)])
+def test_thin_and_ragged_grids_vs_oracle(shape):
+    npy, npx = shape
+    w = W.hump(npx, npy, 10.0, sigma=60.0)
+    new = run_product(w, 60)
+    ref = run_oracle(w, 60, new["k"])
+    assert_parity(new, ref, w.p.epsilon_h)
+
+
+@pytest.mark.parametrize("t_series", [400.0, 20.0])
+def test_boundary_series_vs_oracle(t_series):
+    """N-wave through the CC series, both while it is active and after it
+    expires (t >= tCC[timeCC-2] turns the boundary into a wall)."""
+    w = W.nwave_shelf(96, 64, 50.0, slr=0.5, amp=2.0, period=300.0, t_series=t_series)
+    new = run_product(w, 150)
+    ref = run_oracle(w, 150, new["k"])
+    assert_parity(new, ref, w.p.epsilon_h)
+
+
+def test_periodic_with_series_vs_oracle():
+    w = W.nwave_shelf(40, 36, 50.0, slr=0.5, amp=1.0, period=300.0, t_series=200.0)
+    sw = make_switches(order=2, wbc=2, read_files=1)
+    new = run_product(w, 80, sw)
+    ref = run_oracle(w, 80, new["k"], sw)
+    assert_parity(new, ref, w.p.epsilon_h)
+
+
+def test_run_until_matches_reference_loop():
+    """tsu_run_until steps while t < t_end exactly like GPU/main_TSUNER.cu:157."""
+    w = W.hump(48, 40, 10.0, sigma=80.0)
+    s = T.solver_for(w)
+    n = s.run_until(7.3)
+    t, dt, steps = s.time()
+    V = s.state()
+    s.close()
+    r = oracle.OracleRun(w.p, w.sw, w.V, w.mask, kconsts=run_product(w, 0)["k"])
+    r.run(-1, 7.3)
+    assert n == r.steps == steps
+    assert t == r.t.value and t >= 7.3 and t - dt < 7.3 + dt
+    assert np.array_equal(V, r.V)
+
+
+def test_steps_are_graph_chunk_independent():
+    """16-step CUDA-graph chunks and single launches give identical states."""
+    w = W.hump(64, 64, 10.0, sigma=90.0)
+    a = run_product(w, 37)
+    s = T.solver_for(w)
+    for _ in range(37):
+        s.step(1)
+    V = s.state()
+    s.close()
+    assert np.array_equal(a["V"], V)
+
+
+# ------------------------------------------------ vs the reference CUDA build
+need_ref = pytest.mark.skipif(not oracle.ref_available("default"), reason="oracle/_ref not built")
+
+
+def ref_vs_new(w, nsteps, variant, sw):
+    if not oracle.ref_available(variant):
+        pytest.skip("reference variant %s not built" % variant)
+    CC, tCC = (w.CC, w.tCC) if sw.read_files else (None, None)
+    if variant == "default" and not sw.read_files:
+        CC, tCC = W.expired_series(w.p.npx, w.p.npy)  # Read_files==1 build: walls
+    ref = oracle.ref_run(variant, w.p, w.V, w.mask, CC, tCC, nsteps)
+    new = run_product(w, nsteps, sw)
+    return new, ref
+
+
+@need_ref
+def test_reference_build_switches():
+    assert oracle.ref_switches("default") == dict(order=2, rk=1, wbc=1, bedload=1, suspension=1, read_files=1)
+
+
+@need_ref
+def test_config1_full_vs_reference_build():
+    """512^2, dx=10 m, hump over the noisy 2 % slope, walls, 2000 steps."""
+    w = W.hump(512, 512, 10.0, steps=2000)
+    new, ref = ref_vs_new(w, 2000, "default", make_switches(order=2, wbc=1, read_files=0))
+    assert ref["steps"] == 2000
+    assert_parity(new, ref, w.p.epsilon_h)
+
+
+@need_ref
+def test_nwave_vs_reference_build():
+    w = W.nwave_shelf(160, 96, 25.0, slr=0.5, amp=3.0, period=300.0, t_series=300.0)
+    new, ref = ref_vs_new(w, 300, "default", w.sw)
+    assert_parity(new, ref, w.p.epsilon_h)
+
+
+@need_ref
+def test_config2_slice_4096_vs_reference_build():
+    """Full-size 4096^2 shelf with the N-wave series and harbour mask, 40 steps."""
+    w = W.nwave_shelf(4096, 4096, 5.0)
+    new, ref = ref_vs_new(w, 40, "default", w.sw)
+    assert_parity(new, ref, w.p.epsilon_h)
+
+
+@pytest.mark.parametrize("variant,sw", [
+    ("rf0_wbc1", dict(order=2, wbc=1, read_files=0)),
+    ("rf0_wbc0", dict(order=2, wbc=0, read_files=0)),
+    ("rf0_wbc2", dict(order=2, wbc=2, read_files=0)),
+    ("order1", dict(order=1, wbc=1, read_files=1)),
+    ("nosed", dict(order=2, wbc=1, read_files=1, bedload=0, suspension=0)),
+])
+def test_switch_variants_vs_reference_build(variant, sw):
+    w = W.nwave_shelf(72, 56, 40.0, slr=0.5, amp=2.0, period=300.0, t_series=300.0)
+    w.sw = make_switches(**sw)
+    new, ref = ref_vs_new(w, 150, variant, w.sw)
+    assert_parity(new, ref, w.p.epsilon_h)
+
+
+@need_ref
+def test_oracle_pinned_by_reference_build():
+    """The oracle itself matches the reference CUDA build."""
+    w = W.nwave_shelf(96, 80, 30.0, slr=0.5, amp=2.0, period=300.0, t_series=300.0)
+    ref = oracle.ref_run("default", w.p, w.V, w.mask, w.CC, w.tCC, 120)
+    k = run_product(w, 0)["k"]
+    orc = run_oracle(w, 120, k)
+    assert_parity(orc, ref, w.p.epsilon_h)

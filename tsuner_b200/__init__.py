@@ -1,0 +1,201 @@
+"""tsuner_b200 -- B200-native TSUNER hot path behind a C ABI.
+
+The product is the shared library libtsuner_b200.so (hand-written sm_100a
+CUDA + C++ host code) declared by include/tsuner_b200.h.  This module is a
+thin ctypes binding over that ABI for tests and benchmarks; it has no
+compute of its own and no CPU fallback: if the library is missing or cannot
+be loaded the import of `lib()` raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import (SimParams, TsuConsts, TsuSwitches, TSU_OK, make_params,  # noqa: F401
+                  make_switches, derive_params)
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libtsuner_b200.so")
+_LIB = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+# every symbol include/tsuner_b200.h declares
+EXPORTS = [
+    "TSUNER", "checkCUDAsupport", "initializeGPU",
+    "tsu_switches_default", "tsu_set_default_switches", "tsu_get_default_switches",
+    "tsu_derive_params", "tsu_parse_data_dat",
+    "tsu_create", "tsu_destroy", "tsu_set_state", "tsu_set_mask", "tsu_set_boundary_series",
+    "tsu_reset", "tsu_step", "tsu_run_until", "tsu_sync", "tsu_get_state", "tsu_get_extrema",
+    "tsu_get_time", "tsu_get_consts", "tsu_last_step_ms", "tsu_last_step_launches",
+    "tsu_state_device", "tsu_strerror", "tsu_last_error", "tsu_version", "tsu_struct_sizes",
+]
+
+
+class TsunerError(RuntimeError):
+    def __init__(self, code, what):
+        msg = "%s failed: %s (%d)" % (what, lib().tsu_strerror(code).decode(), code)
+        detail = lib().tsu_last_error()
+        if detail:
+            msg += " -- " + detail.decode()
+        super().__init__(msg)
+        self.code = code
+
+
+def lib():
+    """Loads the product library (raises if it is not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libtsuner_b200.so is not built; run `python -m tsuner_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        sig = {
+            "tsu_switches_default": ([C.POINTER(TsuSwitches)], C.c_int),
+            "tsu_set_default_switches": ([C.POINTER(TsuSwitches)], C.c_int),
+            "tsu_get_default_switches": ([C.POINTER(TsuSwitches)], C.c_int),
+            "tsu_derive_params": ([C.POINTER(SimParams), C.c_double], C.c_int),
+            "tsu_create": ([C.POINTER(vp), C.POINTER(SimParams), C.POINTER(TsuSwitches), C.c_int], C.c_int),
+            "tsu_destroy": ([vp], C.c_int),
+            "tsu_set_state": ([vp, vp, vp, vp, vp, vp], C.c_int),
+            "tsu_set_mask": ([vp, vp], C.c_int),
+            "tsu_set_boundary_series": ([vp, vp, vp, C.c_ulong], C.c_int),
+            "tsu_reset": ([vp], C.c_int),
+            "tsu_step": ([vp, C.c_long], C.c_int),
+            "tsu_run_until": ([vp, C.c_double, C.c_long, C.POINTER(C.c_long)], C.c_int),
+            "tsu_sync": ([vp], C.c_int),
+            "tsu_get_state": ([vp, vp], C.c_int),
+            "tsu_get_extrema": ([vp, vp, vp, vp], C.c_int),
+            "tsu_get_time": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_long)], C.c_int),
+            "tsu_get_consts": ([vp, C.POINTER(TsuConsts)], C.c_int),
+            "tsu_last_step_ms": ([vp, C.POINTER(C.c_double)], C.c_int),
+            "tsu_last_step_launches": ([vp, C.POINTER(C.c_long)], C.c_int),
+            "tsu_state_device": ([vp, C.POINTER(vp), C.POINTER(C.c_long), C.POINTER(C.c_long),
+                                  C.POINTER(C.c_int)], C.c_int),
+            "tsu_strerror": ([C.c_int], C.c_char_p),
+            "tsu_last_error": ([], C.c_char_p),
+            "tsu_version": ([], C.c_char_p),
+            "tsu_struct_sizes": ([C.POINTER(C.c_size_t)], C.c_int),
+            "tsu_parse_data_dat": ([C.c_char_p, C.POINTER(SimParams), C.c_char_p, C.c_char_p, C.c_char_p,
+                                    C.c_char_p, C.POINTER(C.c_double), C.c_char_p, C.c_size_t], C.c_int),
+            "checkCUDAsupport": ([C.c_int], C.c_int),
+            "initializeGPU": ([], None),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _LIB = L
+    return _LIB
+
+
+def _ck(code, what):
+    if code != TSU_OK:
+        raise TsunerError(code, what)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Solver:
+    """One simulation on one GPU through the tsu_* C ABI."""
+
+    def __init__(self, p, sw, device=0):
+        self.p, self.sw = p, sw
+        self._h = C.c_void_p()
+        _ck(lib().tsu_create(C.byref(self._h), C.byref(p), C.byref(sw), device), "tsu_create")
+
+    def close(self):
+        if self._h:
+            lib().tsu_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_state(self, V):
+        V = np.ascontiguousarray(V, np.float64).reshape(5, self.p.npy, self.p.npx)
+        _ck(lib().tsu_set_state(self._h, _p(V[0]), _p(V[1]), _p(V[2]), _p(V[3]), _p(V[4])), "tsu_set_state")
+
+    def set_mask(self, mask):
+        m = None if mask is None else np.ascontiguousarray(mask, np.int32).reshape(-1)
+        _ck(lib().tsu_set_mask(self._h, _p(m)), "tsu_set_mask")
+
+    def set_boundary_series(self, CC, tCC):
+        self._CC = np.ascontiguousarray(CC, np.float64)
+        self._tCC = np.ascontiguousarray(tCC, np.float64)
+        _ck(lib().tsu_set_boundary_series(self._h, _p(self._CC), _p(self._tCC), len(self._tCC)),
+            "tsu_set_boundary_series")
+
+    def reset(self):
+        _ck(lib().tsu_reset(self._h), "tsu_reset")
+
+    def step(self, n):
+        _ck(lib().tsu_step(self._h, n), "tsu_step")
+
+    def run_until(self, t_end, max_steps=1 << 40):
+        n = C.c_long()
+        _ck(lib().tsu_run_until(self._h, t_end, max_steps, C.byref(n)), "tsu_run_until")
+        return n.value
+
+    def sync(self):
+        _ck(lib().tsu_sync(self._h), "tsu_sync")
+
+    def state(self):
+        V = np.empty((5, self.p.npy, self.p.npx))
+        _ck(lib().tsu_get_state(self._h, _p(V)), "tsu_get_state")
+        return V
+
+    def extrema(self):
+        shp = (self.p.npy, self.p.npx)
+        a, b, c = np.empty(shp), np.empty(shp), np.empty(shp)
+        _ck(lib().tsu_get_extrema(self._h, _p(a), _p(b), _p(c)), "tsu_get_extrema")
+        return a, b, c
+
+    def time(self):
+        t, dt, n = C.c_double(), C.c_double(), C.c_long()
+        _ck(lib().tsu_get_time(self._h, C.byref(t), C.byref(dt), C.byref(n)), "tsu_get_time")
+        return t.value, dt.value, n.value
+
+    def consts(self):
+        k = TsuConsts()
+        _ck(lib().tsu_get_consts(self._h, C.byref(k)), "tsu_get_consts")
+        return k
+
+    def last_ms(self):
+        ms = C.c_double()
+        _ck(lib().tsu_last_step_ms(self._h, C.byref(ms)), "tsu_last_step_ms")
+        return ms.value
+
+    def last_launches(self):
+        n = C.c_long()
+        _ck(lib().tsu_last_step_launches(self._h, C.byref(n)), "tsu_last_step_launches")
+        return n.value
+
+    def device_state(self):
+        ptr, pitch, plane, eb = C.c_void_p(), C.c_long(), C.c_long(), C.c_int()
+        _ck(lib().tsu_state_device(self._h, C.byref(ptr), C.byref(pitch), C.byref(plane), C.byref(eb)),
+            "tsu_state_device")
+        return ptr.value, pitch.value, plane.value, eb.value
+
+
+def solver_for(w, device=0):
+    """Solver loaded with a workloads.Workload's state, mask and series."""
+    s = Solver(w.p, w.sw, device)
+    s.set_state(w.V)
+    s.set_mask(w.mask)
+    if w.sw.read_files:
+        s.set_boundary_series(w.CC, w.tCC)
+    s.reset()
+    return s

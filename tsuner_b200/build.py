@@ -1,0 +1,85 @@
+"""Builds the in-tree product library tsuner_b200/libtsuner_b200.so (sm_100a).
+
+  python -m tsuner_b200.build [--force]
+
+Every .cu/.cpp under csrc/ is compiled separately (the FP64 plain-form units
+with -fmad=false, matching the reference build, GPU/makefile:10, so that no
+multiply-add is contracted) and linked into one shared library exporting the
+C ABI of include/tsuner_b200.h.  Objects go to tsuner_b200/_build/.
+"""
+import argparse
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+OBJ = os.path.join(PKG, "_build")
+LIB = os.path.join(PKG, "libtsuner_b200.so")
+INC = os.path.join(ROOT, "include")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+# per-unit extra flags
+UNIT_FLAGS = {
+    "stage64.cu": ["-fmad=false"],
+    "solver.cu": ["-fmad=false"],
+}
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC]
+
+
+def _headers():
+    hs = [os.path.join(INC, f) for f in os.listdir(INC)]
+    hs += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    return hs
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError("build failed: " + os.path.basename(cmd[-3] if len(cmd) > 3 else cmd[0]))
+    return r
+
+
+def build(force=False, verbose=False):
+    os.makedirs(OBJ, exist_ok=True)
+    srcs = sorted(f for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
+    hdrs = _headers() + [os.path.abspath(__file__)]
+    objs = []
+    for f in srcs:
+        src = os.path.join(CSRC, f)
+        obj = os.path.join(OBJ, f + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [src] + hdrs):
+            cmd = [NVCC] + ARCH + COMMON + UNIT_FLAGS.get(f, []) + ["-c", src, "-o", obj]
+            if f.endswith(".cpp"):
+                cmd = [NVCC] + COMMON + ["-x", "c++", "-c", src, "-o", obj]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            r = _run(cmd)
+            if verbose:
+                sys.stdout.write(r.stderr)
+    if force or _stale(LIB, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+    return LIB
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("-v", "--verbose", action="store_true")
+    a = ap.parse_args(argv)
+    print(build(a.force, a.verbose))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,221 @@
+// physics64.cuh -- FP64 point physics of the TSUNER scheme, evaluated in the
+// reference's exact operation order so that the fused kernels reproduce the
+// reference CUDA build bit for bit (both are compiled with -fmad=false, and
+// double division and sqrt are IEEE round-to-nearest on the device).
+//
+// What differs from the reference is WHERE things are computed, not how:
+// per-run constants (settling velocity, pow() terms, sqrt(FR), sqrt(OC)) are
+// evaluated once per run with the reference expressions (TsuConsts), cell
+// velocities are evaluated once per cell instead of five times, and face
+// states / edge fluxes never leave shared memory.
+#pragma once
+#include <cfloat>
+#include <cstdint>
+
+#include "tsuner_b200.h"
+
+namespace tsu {
+
+constexpr double kG = 9.81;              // Sim_parameters.hxx:34
+constexpr double kEpsilon = DBL_EPSILON; // Sim_parameters.hxx:28
+constexpr double kEps = 1e-6;            // Sim_parameters.hxx:35
+constexpr double kVmax = 10.0;           // Sim_parameters.hxx:36
+
+// Scalar parameters the stage kernels need, packed once per run.
+struct Phys64 {
+    double FR, eps_h, Opar, OC, Q, HQB, porosity, CFL, dx, dy, inv_dx, inv_dy;
+    TsuConsts k;
+    int npx, npy;
+    int order, wbc, bedload, suspension, read_files, bedload_law;
+    double grass_ag;
+};
+
+// SGN (Sim_parameters.hxx:29)
+__device__ __forceinline__ int sgn(double x) { return (fabs(x) < kEpsilon) ? 0 : ((x) > 0) ? 1 : -1; }
+
+// u_calculator_double (GPU/SedFlux.cuh:39-49)
+__device__ __forceinline__ void velocity(double h, double qx, double qy, double &ux, double &uy) {
+    double u = qx / (h + kEpsilon) * (double)(h >= kEps);
+    double v = qy / (h + kEpsilon) * (double)(h >= kEps);
+    double modu = sqrt(u * u + v * v);
+    if (modu > kVmax) {
+        u = u / modu * kVmax;
+        v = v / modu * kVmax;
+    }
+    ux = u;
+    uy = v;
+}
+
+// avg, the van-Leer-type limiter (GPU/Reconstructor.cu:19-31)
+__device__ __forceinline__ double limiter(double a, double b) {
+    double aa = fabs(a), bb = fabs(b);
+    return ((aa + bb) > kEpsilon) ? (a * bb + b * aa) / (aa + bb) : 0.0;
+}
+
+// state_filter_double (GPU/SedFlux.cuh:118-132)
+__device__ __forceinline__ void positivity_filter(double &h, double &qx, double &qy, double &hc) {
+    h = h * (double)(h > 0.0);
+    double c = hc / (h + kEpsilon);
+    c = c * (double)(c > 0.0);
+    double ux, uy;
+    velocity(h, qx, qy, ux, uy);
+    qx = h * ux;
+    qy = h * uy;
+    hc = h * c;
+}
+
+struct State5 {
+    double h, qx, qy, H, hc;
+};
+
+// bedload (GPU/SedFlux.cuh:150-168), or the Grass law when selected.
+__device__ __forceinline__ double bedload_flux(const Phys64 &P, double h, double ux, double uy) {
+    double modu = sqrt(ux * ux + uy * uy);
+    if (P.bedload_law == 1) return -(P.grass_ag * ux * modu * modu / (1.0 - P.porosity));
+    double O = P.Opar * modu * modu;
+    double K1 = 17.0 * ux / (modu + kEpsilon);
+    double qb = K1 * P.Q * fmax(O - P.OC, 0.0) * fmax(sqrt(O) - P.k.sqrt_OC, 0.0) *
+                (double)(h > P.HQB) * (double)(h > P.k.DS5);
+    return -qb;
+}
+
+// Cflux (GPU/SedFlux.cuh:171-179)
+__device__ __forceinline__ void phys_flux(const Phys64 &P, double h, double ux, double uy, double hc,
+                                          int fixed, double F[5]) {
+    F[0] = h * ux;
+    F[1] = F[0] * ux;
+    F[2] = F[0] * uy;
+    F[3] = bedload_flux(P, h, ux, uy) * (double)fixed * (double)P.bedload;
+    F[4] = hc * ux;
+}
+
+// One edge: RiemannSolver_Vols (GPU/VolumeSolver.cu:19-126) with the
+// rotation back of :129-152.  `a` is the state on the side the normal leaves
+// (index 0 in the reference), `b` the state it enters.  Dm is the
+// fluctuation into side a, Dp into side b, both in x/y components.
+__device__ __forceinline__ void edge_flux(const Phys64 &P, const State5 &a, const State5 &b, int nx, int ny,
+                                          int fixed, double Dm[5], double Dp[5]) {
+    const double dnx = (double)nx, dny = (double)ny;
+    double qlx = a.qx * dnx + a.qy * dny;
+    double qly = a.qy * dnx - a.qx * dny;
+    double qrx = b.qx * dnx + b.qy * dny;
+    double qry = b.qy * dnx - b.qx * dny;
+    double u0x, u0y, u1x, u1y;
+    velocity(a.h, qlx, qly, u0x, u0y);
+    velocity(b.h, qrx, qry, u1x, u1y);
+    double c0 = a.hc / (a.h + kEpsilon);
+    double c1 = b.hc / (b.h + kEpsilon);
+
+    // hydrostatic reconstruction (:37-40)
+    double zmH = fmin(a.H, b.H);
+    double h0 = fmax(a.h - a.H + zmH, 0.0);
+    double h1 = fmax(b.h - b.H + zmH, 0.0);
+    double q0x = u0x * h0, q0y = u0y * h0;
+    double q1x = u1x * h1, q1y = u1y * h1;
+    double hc0 = h0 * c0, hc1 = h1 * c1;
+    double deta = h1 - h0;
+
+    double F0[5], F1[5];
+    phys_flux(P, h0, u0x, u0y, hc0, fixed, F0);
+    phys_flux(P, h1, u1x, u1y, hc1, fixed, F1);
+
+    // Roe average + wave-speed bounds (GPU/SedFlux.cuh:181-199)
+    double hm = 0.5 * (h0 + h1);
+    double s0q = sqrt(h0), s1q = sqrt(h1);
+    double umx = (s0q * u0x + s1q * u1x) / (s0q + s1q);
+    double SL = u0x - sqrt(kG * h0);
+    double SR = u1x + sqrt(kG * h1);
+    double cm = sqrt(kG * hm);
+    SL = fmin(SL, umx - cm);
+    SR = fmax(SR, umx + cm);
+
+    double a0, a1;
+    if (SR - SL > kEpsilon) {
+        a0 = (SR * fabs(SL) - SL * fabs(SR)) / (SR - SL);
+        a1 = (fabs(SR) - fabs(SL)) / (SR - SL);
+    } else {
+        a0 = fmax(fabs(SL), fabs(SR));
+        a1 = 0.0;
+    }
+
+    double df[5], DU[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) df[i] = F1[i] - F0[i];
+    df[1] += kG * hm * deta;
+    DU[0] = h1 - h0;
+    DU[1] = q1x - q0x;
+    DU[2] = q1y - q0y;
+    DU[3] = b.H - a.H;
+    DU[4] = hc1 - hc0;
+    double s0 = sgn(b.H - a.H);
+    double s1 = sgn(df[3]);
+    double s2 = sgn(a1);
+    if (fabs(s0) > kEpsilon) s1 = s1 / s0;
+    else s1 = 0.0;
+    double vis[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) vis[i] = a0 * DU[i] + a1 * df[i];
+    if (s2 == s1) vis[3] = a1 * df[3];
+    else vis[3] = -a1 * df[3];
+    double m[5], p[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) {
+        m[i] = 0.5 * (df[i] - vis[i]) + F0[i];
+        p[i] = 0.5 * (df[i] + vis[i]) - F1[i];
+    }
+    Dm[0] = m[0];
+    Dm[1] = (dnx * m[1] - dny * m[2]);
+    Dm[2] = (dny * m[1] + dnx * m[2]);
+    Dm[3] = m[3];
+    Dm[4] = m[4];
+    Dp[0] = p[0];
+    Dp[1] = (dnx * p[1] - dny * p[2]);
+    Dp[2] = (dny * p[1] + dnx * p[2]);
+    Dp[3] = p[3];
+    Dp[4] = p[4];
+}
+
+// interpolate_time (GPU/VolumeSolver.cu:172-203): boundary state from the
+// CC series at segment `seg`; replaces h, H, qx, qy and zeroes hc.
+__device__ __forceinline__ void series_state(const double *__restrict__ CC, const double *__restrict__ tCC,
+                                             double t, int npx, int npy, int seg, State5 &g) {
+    double dt = tCC[1] - tCC[0];
+    int it = int((t - tCC[0]) / dt);
+    it *= (it > 0);
+    int tp = it + 1;
+    long long nseg4 = (long long)(2 * npx + 2 * npy) * 4;
+    long long posCC = it * nseg4 + (long long)seg * 4;
+    long long posCCp = tp * nseg4 + (long long)seg * 4;
+    double m = (CC[posCCp] - CC[posCC]) / dt;
+    double b = CC[posCC] - m * tCC[it];
+    double h1 = m * t + b;
+    m = (CC[posCCp + 3] - CC[posCC + 3]) / dt;
+    b = CC[posCC + 3] - m * tCC[it];
+    double zb1 = m * t + b;
+    h1 += zb1;
+    m = (CC[posCCp + 1] - CC[posCC + 1]) / dt;
+    b = CC[posCC + 1] - m * tCC[it];
+    double qx = m * t + b;
+    qx *= h1;
+    m = (CC[posCCp + 2] - CC[posCC + 2]) / dt;
+    b = CC[posCC + 2] - m * tCC[it];
+    double qy = m * t + b;
+    qy *= h1;
+    g.h = h1;
+    g.H = zb1;
+    g.qx = qx;
+    g.qy = qy;
+    g.hc = 0.0;
+}
+
+// GetDeltaT per cell (GPU/Volume_kernel.cu:28-41)
+__device__ __forceinline__ double cfl_dt(const Phys64 &P, double h, double qx, double qy) {
+    double ux, uy;
+    velocity(h, qx, qy, ux, uy);
+    double cg = sqrt(kG * h);
+    double lx = fabs(ux) + cg;
+    double ly = fabs(uy) + cg;
+    return P.CFL * 0.5 * fmin(P.dx / lx, P.dy / ly);
+}
+
+}  // namespace tsu

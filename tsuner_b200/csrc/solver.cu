@@ -1,0 +1,514 @@
+// solver.cu -- TsuSolver: device buffers, stepping and the tsu_* C ABI.
+//
+// Device layout (HBM): each field is a plane of npy rows with a row pitch
+// rounded up to 32 elements (256 B for FP64), planes consecutive:
+//   bufA  [5][npy][pitch]  U^n at step entry / U^{n+1} at exit
+//   bufB  [5][npy][pitch]  U* (intermediate RK stage)
+//   hmax, bmin, eta_max [npy][pitch], mask [npy][pitch] uint8
+// About 105 B per cell in FP64 (the reference allocates ~796 B per cell,
+// GPU/main_TSUNER.cu:57-91).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "solver.h"
+#include "stage64.h"
+#include "tsuner_b200.h"
+
+using namespace tsu;
+
+namespace {
+thread_local char g_err[512] = "";
+std::mutex g_defaults_mu;
+TsuSwitches g_defaults = {2, 1, 1, 1, 1, 1, 0, 0, 1e-3};
+
+int cuda_fail(cudaError_t e, const char *what) {
+    snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
+    return (e == cudaErrorMemoryAllocation) ? TSU_ERR_GPU_OOM : TSU_ERR_CUDA;
+}
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t _e = (call);                              \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call);   \
+    } while (0)
+
+__global__ void set_scal_kernel(double *scal, int i, double v) { scal[i] = v; }
+}  // namespace
+
+const char *tsu_last_error_detail() { return g_err; }
+
+static int validate(const SimParams *p, const TsuSwitches *sw) {
+    if (!p || !sw) return TSU_ERR_INVALID;
+    if (p->npx < 1 || p->npy < 1 || (long long)p->npx * p->npy > (1LL << 31) - 1) return TSU_ERR_INVALID;
+    if (!(p->dx > 0) || !(p->dy > 0) || !(p->CFL > 0)) return TSU_ERR_INVALID;
+    if (sw->order != 1 && sw->order != 2) return TSU_ERR_INVALID;
+    if (sw->rk != 1) return TSU_ERR_INVALID;
+    if (sw->wbc < 0 || sw->wbc > 2) return TSU_ERR_INVALID;
+    if (sw->bedload_law < 0 || sw->bedload_law > 1) return TSU_ERR_INVALID;
+    if (sw->precision != 0) return TSU_ERR_INVALID;
+    return TSU_OK;
+}
+
+extern "C" int tsu_switches_default(TsuSwitches *sw) {
+    if (!sw) return TSU_ERR_INVALID;
+    TsuSwitches d = {2, 1, 1, 1, 1, 1, 0, 0, 1e-3};
+    *sw = d;
+    return TSU_OK;
+}
+extern "C" int tsu_set_default_switches(const TsuSwitches *sw) {
+    if (!sw) return TSU_ERR_INVALID;
+    std::lock_guard<std::mutex> g(g_defaults_mu);
+    g_defaults = *sw;
+    return TSU_OK;
+}
+extern "C" int tsu_get_default_switches(TsuSwitches *sw) {
+    if (!sw) return TSU_ERR_INVALID;
+    std::lock_guard<std::mutex> g(g_defaults_mu);
+    *sw = g_defaults;
+    return TSU_OK;
+}
+
+extern "C" int tsu_derive_params(SimParams *p, double friction_datdat) {
+    if (!p) return TSU_ERR_INVALID;
+    p->FR = friction_datdat / 8.0;  // Problem_loader.cxx:337-339 (Chezy)
+    p->HQB = 5.0 * p->DS;
+    p->Q = p->DS * sqrt(9.81 * (p->R - 1.0) * p->DS) / (1.0 - p->porosity);
+    p->Opar = p->FR / ((p->R - 1.0) * 9.81 * p->DS);
+    return TSU_OK;
+}
+
+static void free_all(TsuSolver *s) {
+    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    cudaFree(s->A);
+    cudaFree(s->B);
+    cudaFree(s->hmax);
+    cudaFree(s->bmin);
+    cudaFree(s->eta);
+    cudaFree(s->mask);
+    cudaFree(s->CC);
+    cudaFree(s->tCC);
+    cudaFree(s->scal);
+    cudaFree(s->partials);
+    cudaFree(s->ticket);
+    cudaFree(s->dconsts);
+    if (s->e0) cudaEventDestroy(s->e0);
+    if (s->e1) cudaEventDestroy(s->e1);
+    if (s->st) cudaStreamDestroy(s->st);
+}
+
+extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches *sw, int device) {
+    if (!out) return TSU_ERR_INVALID;
+    *out = nullptr;
+    int rc = validate(p, sw);
+    if (rc) {
+        snprintf(g_err, sizeof(g_err), "invalid parameters or switches");
+        return rc;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        snprintf(g_err, sizeof(g_err), "no CUDA device");
+        return TSU_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return TSU_ERR_NO_DEVICE;
+    CK(cudaSetDevice(device));
+    TsuSolver *s = new (std::nothrow) TsuSolver();
+    if (!s) return TSU_ERR_HOST_OOM;
+    s->p = *p;
+    s->p.nvol = p->npx * p->npy;
+    s->sw = *sw;
+    s->device = device;
+    s->pitch = ((long long)p->npx + 31) / 32 * 32;
+    s->plane = s->pitch * p->npy;
+    const size_t pl = (size_t)s->plane * sizeof(double);
+    cudaError_t e = cudaSuccess;
+#define AL(ptr, bytes)                                            \
+    if (e == cudaSuccess) e = cudaMalloc((void **)&(ptr), (bytes));
+    AL(s->A, 5 * pl);
+    AL(s->B, 5 * pl);
+    AL(s->hmax, pl);
+    AL(s->bmin, pl);
+    AL(s->eta, pl);
+    AL(s->mask, (size_t)s->plane);
+    AL(s->scal, SC_N * sizeof(double));
+    s->npartials = partials_needed(p->npx, p->npy);
+    AL(s->partials, s->npartials * sizeof(double));
+    AL(s->ticket, sizeof(unsigned));
+    AL(s->dconsts, sizeof(TsuConsts));
+#undef AL
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->e1);
+    if (e == cudaSuccess) e = stage64_prepare();
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->A, 0, 5 * pl, s->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->B, 0, 5 * pl, s->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->mask, 1, (size_t)s->plane, s->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->ticket, 0, sizeof(unsigned), s->st);
+    if (e == cudaSuccess) e = consts_launch(s->p, s->dconsts, s->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&s->hconsts, s->dconsts, sizeof(TsuConsts), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) {
+        int r = cuda_fail(e, "tsu_create");
+        free_all(s);
+        delete s;
+        return r;
+    }
+    Phys64 &P = s->phys;
+    P.FR = p->FR;
+    P.eps_h = p->epsilon_h;
+    P.Opar = p->Opar;
+    P.OC = p->OC;
+    P.Q = p->Q;
+    P.HQB = p->HQB;
+    P.porosity = p->porosity;
+    P.CFL = p->CFL;
+    P.dx = p->dx;
+    P.dy = p->dy;
+    P.inv_dx = 1.0 / p->dx;  // GPU/main_TSUNER.cu:43-44
+    P.inv_dy = 1.0 / p->dy;
+    P.k = s->hconsts;
+    P.npx = p->npx;
+    P.npy = p->npy;
+    P.order = sw->order;
+    P.wbc = sw->wbc;
+    P.bedload = sw->bedload;
+    P.suspension = sw->suspension;
+    P.read_files = sw->read_files;
+    P.bedload_law = sw->bedload_law;
+    P.grass_ag = sw->grass_ag;
+    *out = s;
+    return TSU_OK;
+}
+
+extern "C" int tsu_destroy(TsuSolver *s) {
+    if (!s) return TSU_OK;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->st);
+    free_all(s);
+    delete s;
+    return TSU_OK;
+}
+
+static int upload_plane(TsuSolver *s, double *dst, const double *src) {
+    CK(cudaMemcpy2DAsync(dst, s->pitch * sizeof(double), src, s->p.npx * sizeof(double),
+                         s->p.npx * sizeof(double), s->p.npy, cudaMemcpyHostToDevice, s->st));
+    return TSU_OK;
+}
+
+extern "C" int tsu_set_state(TsuSolver *s, const double *h, const double *qx, const double *qy, const double *H,
+                             const double *hc) {
+    if (!s || !h || !qx || !qy || !H) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    const double *src[5] = {h, qx, qy, H, hc};
+    for (int f = 0; f < 5; f++) {
+        double *dst = s->A + f * s->plane;
+        if (src[f]) {
+            int r = upload_plane(s, dst, src[f]);
+            if (r) return r;
+        } else {
+            CK(cudaMemsetAsync(dst, 0, (size_t)s->plane * sizeof(double), s->st));
+        }
+    }
+    CK(cudaStreamSynchronize(s->st));
+    s->has_state = true;
+    s->ready = false;
+    return TSU_OK;
+}
+
+extern "C" int tsu_set_mask(TsuSolver *s, const int *fixH) {
+    if (!s) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    if (!fixH) {
+        CK(cudaMemsetAsync(s->mask, 1, (size_t)s->plane, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        return TSU_OK;
+    }
+    const long long n = (long long)s->p.npx * s->p.npy;
+    std::vector<unsigned char> m;
+    try {
+        m.resize((size_t)n);
+    } catch (...) {
+        return TSU_ERR_HOST_OOM;
+    }
+    for (long long i = 0; i < n; i++) {
+        if (fixH[i] != 0 && fixH[i] != 1) {
+            snprintf(g_err, sizeof(g_err), "mask value %d at %lld is not 0 or 1", fixH[i], i);
+            return TSU_ERR_INVALID;
+        }
+        m[(size_t)i] = (unsigned char)fixH[i];
+    }
+    CK(cudaMemcpy2DAsync(s->mask, s->pitch, m.data(), s->p.npx, s->p.npx, s->p.npy, cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return TSU_OK;
+}
+
+extern "C" int tsu_set_boundary_series(TsuSolver *s, const double *CC, const double *tCC, unsigned long timeCC) {
+    if (!s || !CC || !tCC || timeCC < 2) return TSU_ERR_INVALID;
+    // GPU/VolumeSolver.cu:172-215 assumes a uniform series; check it so that
+    // interpolation indices stay inside the arrays.
+    double dtc = tCC[1] - tCC[0];
+    if (!(dtc > 0)) return TSU_ERR_INVALID;
+    for (unsigned long q = 1; q < timeCC; q++)
+        if (fabs((tCC[q] - tCC[0]) - q * dtc) > 1e-9 * fabs(dtc) * q) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    cudaFree(s->CC);
+    cudaFree(s->tCC);
+    s->CC = s->tCC = nullptr;
+    size_t n = (size_t)(2 * s->p.npx + 2 * s->p.npy) * 4 * timeCC;
+    CK(cudaMalloc((void **)&s->CC, n * sizeof(double)));
+    CK(cudaMalloc((void **)&s->tCC, timeCC * sizeof(double)));
+    CK(cudaMemcpyAsync(s->CC, CC, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->tCC, tCC, timeCC * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    s->timeCC = timeCC;
+    s->invalidate_graph();
+    return TSU_OK;
+}
+
+Stage64Args TsuSolver::args() const {
+    Stage64Args a;
+    a.bufA = A;
+    a.bufB = B;
+    a.mask = mask;
+    a.CC = CC;
+    a.tCC = tCC;
+    a.timeCC = timeCC;
+    a.hmax = hmax;
+    a.bmin = bmin;
+    a.eta_max = eta;
+    a.scal = scal;
+    a.partials = partials;
+    a.ticket = ticket;
+    a.pitch = pitch;
+    a.plane = plane;
+    a.phys = phys;
+    return a;
+}
+
+void TsuSolver::invalidate_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    graph_exec = nullptr;
+    graph = nullptr;
+}
+
+extern "C" int tsu_reset(TsuSolver *s) {
+    if (!s || !s->has_state) return TSU_ERR_INVALID;
+    if (s->sw.read_files && s->timeCC < 2) {
+        snprintf(g_err, sizeof(g_err), "read_files is set but no boundary series was given");
+        return TSU_ERR_INVALID;
+    }
+    CK(cudaSetDevice(s->device));
+    double init[SC_N] = {0.0, -1.0, HUGE_VAL, 0.0, 0.0, 0.0, 0.0, 0.0};
+    CK(cudaMemcpyAsync(s->scal, init, sizeof(init), cudaMemcpyHostToDevice, s->st));
+    CK(fill_launch(s->hmax, s->plane, -1e30, s->st));  // set_inicializacion*, GPU/Volume_kernel.cu:112-137
+    CK(fill_launch(s->bmin, s->plane, -1e30, s->st));
+    CK(fill_launch(s->eta, s->plane, -1e30, s->st));
+    CK(initial_dt_launch(s->A, s->pitch, s->plane, s->phys, s->partials, s->ticket, s->scal, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    s->ready = true;
+    return TSU_OK;
+}
+
+int TsuSolver::launch_steps(long n) {
+    Stage64Args a = args();
+    for (long i = 0; i < n; i++)
+        for (int k = 0; k < sw.order; k++) CK(stage64_launch(sw.order, k, a, st));
+    return TSU_OK;
+}
+
+extern "C" int tsu_step(TsuSolver *s, long nsteps) {
+    if (!s || nsteps < 0) return TSU_ERR_INVALID;
+    if (!s->ready) {
+        int r = tsu_reset(s);
+        if (r) return r;
+    }
+    CK(cudaSetDevice(s->device));
+    CK(cudaEventRecord(s->e0, s->st));
+    long n = nsteps;
+    const long K = TsuSolver::kGraphSteps;
+    if (n >= K && !s->graph_exec) {
+        CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+        int r = s->launch_steps(K);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(s->st, &g);
+        if (r) return r;
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        s->graph = g;
+        CK(cudaGraphInstantiate(&s->graph_exec, g, 0));
+    }
+    while (n >= K && s->graph_exec) {
+        CK(cudaGraphLaunch(s->graph_exec, s->st));
+        n -= K;
+    }
+    int r = s->launch_steps(n);
+    if (r) return r;
+    CK(cudaEventRecord(s->e1, s->st));
+    s->last_launches = nsteps * s->sw.order;
+    s->timed = true;
+    return TSU_OK;
+}
+
+extern "C" int tsu_sync(TsuSolver *s) {
+    if (!s) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->st));
+    return TSU_OK;
+}
+
+extern "C" int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *steps_done) {
+    if (!s || max_steps < 0) return TSU_ERR_INVALID;
+    if (!s->ready) {
+        int r = tsu_reset(s);
+        if (r) return r;
+    }
+    CK(cudaSetDevice(s->device));
+    double sc[SC_N];
+    CK(cudaMemcpy(sc, s->scal, sizeof(sc), cudaMemcpyDeviceToHost));
+    const double steps0 = sc[SC_STEPS];
+    set_scal_kernel<<<1, 1, 0, s->st>>>(s->scal, SC_TEND, t_end);
+    CK(cudaGetLastError());
+    long left = max_steps;
+    while (left > 0) {
+        long chunk = left < 64 ? left : 64;
+        int r = tsu_step(s, chunk);
+        if (r) return r;
+        left -= chunk;
+        CK(cudaMemcpyAsync(sc, s->scal, sizeof(sc), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        if (!(sc[SC_T] < t_end)) break;
+    }
+    set_scal_kernel<<<1, 1, 0, s->st>>>(s->scal, SC_TEND, HUGE_VAL);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->st));
+    if (steps_done) *steps_done = (long)(sc[SC_STEPS] - steps0);
+    return TSU_OK;
+}
+
+double *TsuSolver::current() const {
+    if (sw.order == 2) return A;
+    double sc[SC_N];
+    if (cudaMemcpy(sc, scal, sizeof(sc), cudaMemcpyDeviceToHost) != cudaSuccess) return A;
+    return sc[SC_PAR] != 0.0 ? B : A;
+}
+
+extern "C" int tsu_get_state(TsuSolver *s, double *V) {
+    if (!s || !V) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->st));
+    const double *cur = s->current();
+    const size_t n = (size_t)s->p.npx * s->p.npy;
+    for (int f = 0; f < 5; f++)
+        CK(cudaMemcpy2D(V + f * n, s->p.npx * sizeof(double), cur + f * s->plane, s->pitch * sizeof(double),
+                        s->p.npx * sizeof(double), s->p.npy, cudaMemcpyDeviceToHost));
+    return TSU_OK;
+}
+
+extern "C" int tsu_get_extrema(TsuSolver *s, double *hmax, double *bmin, double *eta_max) {
+    if (!s) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->st));
+    double *src[3] = {s->hmax, s->bmin, s->eta};
+    double *dst[3] = {hmax, bmin, eta_max};
+    for (int f = 0; f < 3; f++)
+        if (dst[f])
+            CK(cudaMemcpy2D(dst[f], s->p.npx * sizeof(double), src[f], s->pitch * sizeof(double),
+                            s->p.npx * sizeof(double), s->p.npy, cudaMemcpyDeviceToHost));
+    return TSU_OK;
+}
+
+extern "C" int tsu_get_time(TsuSolver *s, double *t, double *dt, long *steps) {
+    if (!s) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->st));
+    double sc[SC_N];
+    CK(cudaMemcpy(sc, s->scal, sizeof(sc), cudaMemcpyDeviceToHost));
+    if (t) *t = sc[SC_T];
+    if (dt) *dt = sc[SC_DT];
+    if (steps) *steps = (long)sc[SC_STEPS];
+    return TSU_OK;
+}
+
+extern "C" int tsu_get_consts(TsuSolver *s, TsuConsts *k) {
+    if (!s || !k) return TSU_ERR_INVALID;
+    *k = s->hconsts;
+    return TSU_OK;
+}
+
+extern "C" int tsu_last_step_ms(TsuSolver *s, double *ms) {
+    if (!s || !ms || !s->timed) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    CK(cudaEventSynchronize(s->e1));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, s->e0, s->e1));
+    *ms = f;
+    return TSU_OK;
+}
+
+extern "C" int tsu_last_step_launches(TsuSolver *s, long *launches) {
+    if (!s || !launches) return TSU_ERR_INVALID;
+    *launches = s->last_launches;
+    return TSU_OK;
+}
+
+extern "C" int tsu_state_device(TsuSolver *s, void **ptr, long *pitch_elems, long *plane_elems, int *elem_bytes) {
+    if (!s) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->st));
+    if (ptr) *ptr = s->current();
+    if (pitch_elems) *pitch_elems = (long)s->pitch;
+    if (plane_elems) *plane_elems = (long)s->plane;
+    if (elem_bytes) *elem_bytes = 8;
+    return TSU_OK;
+}
+
+extern "C" const char *tsu_strerror(int code) {
+    switch (code) {
+        case TSU_OK: return "ok";
+        case TSU_ERR_GPU_OOM: return "not enough GPU memory";
+        case TSU_ERR_HOST_OOM: return "not enough CPU memory";
+        case TSU_ERR_INVALID: return "invalid argument";
+        case TSU_ERR_CUDA: return "CUDA runtime error";
+        case TSU_ERR_NO_DEVICE: return "no usable CUDA device";
+        case TSU_ERR_NONFINITE: return "non-finite state";
+        case TSU_ERR_IO: return "output file error";
+        default: return "unknown error";
+    }
+}
+
+extern "C" const char *tsu_last_error(void) { return g_err; }
+
+extern "C" int tsu_struct_sizes(size_t out[3]) {
+    if (!out) return TSU_ERR_INVALID;
+    out[0] = sizeof(SimParams);
+    out[1] = sizeof(TsuSwitches);
+    out[2] = sizeof(TsuConsts);
+    return TSU_OK;
+}
+
+extern "C" const char *tsu_version(void) { return "tsuner_b200 0.1 (sm_100a)"; }
+
+// GPU/CheckCUDASupport.cu:21-44 contract: 0 ok, 1 no GPU, 2 no CUDA GPU, 3 bad index.
+extern "C" int checkCUDAsupport(int cudaDevice) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    if (n == 0) return 1;
+    if (cudaDevice < 0 || cudaDevice >= n) return 3;
+    for (int d = 0; d < n; d++) {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, d) == cudaSuccess && prop.major >= 1) return 0;
+    }
+    return 2;
+}
+
+extern "C" void initializeGPU(void) { cudaFree(0); }

@@ -1,0 +1,57 @@
+// stage64.h -- launch interface of the FP64 fused stage kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "physics64.cuh"
+
+#ifndef S64_TX
+#define S64_TX 32
+#endif
+#ifndef S64_TY
+#define S64_TY 8
+#endif
+
+namespace tsu {
+
+// Device scalars (double slots of Stage64Args::scal):
+//   [0] simulated time t      [1] dt of the next step
+//   [2] t_end of run_until (steps execute only while t < t_end)
+//   [3] steps taken           [4] order-1 ping-pong parity
+enum { SC_T = 0, SC_DT = 1, SC_TEND = 2, SC_STEPS = 3, SC_PAR = 4, SC_N = 8 };
+
+struct Stage64Args {
+    double *bufA;           // U^n at step entry (and U^{n+1} at exit, order 2)
+    double *bufB;           // U* (order 2) / ping-pong partner (order 1)
+    const unsigned char *mask;
+    const double *CC;
+    const double *tCC;
+    unsigned long timeCC;
+    double *hmax, *bmin, *eta_max;
+    double *scal;
+    double *partials;
+    unsigned *ticket;
+    long long pitch, plane;  // elements
+    Phys64 phys;
+};
+
+// dt finalisation of MinReduction<double> (GPU/Reduction_kernel_min.cu:
+// 155-196): above 4096 cells every device compare is fminf on doubles, so
+// the minimum is rounded to float; the host loop starts from 1e30.
+__device__ __forceinline__ double finalize_dt(double m, long long ncells) {
+    if (ncells > 4096) m = (double)__double2float_rn(m);
+    if (!(m < 1e30)) m = 1e30;
+    return m;
+}
+
+size_t stage64_smem_bytes();
+cudaError_t stage64_prepare();
+dim3 stage64_grid(int npx, int npy);
+cudaError_t stage64_launch(int order, int stage, const Stage64Args &a, cudaStream_t st);
+cudaError_t initial_dt_launch(const double *V, long long pitch, long long plane, const Phys64 &P, double *partials,
+                              unsigned *ticket, double *scal, cudaStream_t st);
+cudaError_t fill_launch(double *p, long long n, double v, cudaStream_t st);
+cudaError_t consts_launch(const SimParams &p, TsuConsts *k, cudaStream_t st);
+size_t partials_needed(int npx, int npy);
+
+}  // namespace tsu
