@@ -37,10 +37,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Mcell-steps/s: FP32 fused vs FP64 plain at stated L-inf error; % HBM peak"
-# algorithmic DRAM bytes per cell-step of the fused FP64 form, 5 state planes:
+# algorithmic DRAM bytes per cell-step of the fused forms, 5 state planes:
 # stage 1 reads U^n, writes U*; stage 2 reads U* and U^n, writes U^{n+1}
-# (5 x 5 planes x 8 B), mask read twice (2 x 1 B), hmax/bmin/eta_max RMW (48 B)
-BYTES_PER_CELL_STEP = {"f64": 5 * 5 * 8 + 2 + 3 * 16}
+# (5 x 5 planes x element size), mask read twice (2 x 1 B), hmax/bmin/eta_max
+# read-modify-write (3 x 2 x element size)
+BYTES_PER_CELL_STEP = {"f64": 5 * 5 * 8 + 2 + 3 * 16, "f32": 5 * 5 * 4 + 2 + 3 * 8}
 
 
 def peaks():
@@ -181,15 +182,14 @@ def traffic_from_profiles(name):
     return None
 
 
-def run_ours(a, rank, world, local, dist):
-    import tsuner_b200 as T
-    w, desc = workload(a.workload)
-    n = w.ncells
-    s = T.Solver(w.p, w.sw, device=local)
-    # ---- device-timed region (inputs resident in HBM)
+def timed_form(T, w, sw, a, local, dist):
+    """W warm-up steps, then K device-timed steps (CUDA events on the solver's
+    stream, barrier + sync on both sides).  Returns the solver (state after
+    W + K steps) and the timing."""
+    s = T.Solver(w.p, sw, device=local)
     s.set_state(w.V)
     s.set_mask(w.mask)
-    if w.sw.read_files:
+    if sw.read_files:
         s.set_boundary_series(w.CC, w.tCC)
     s.reset()
     s.step(a.warmup)
@@ -199,8 +199,27 @@ def run_ours(a, rank, world, local, dist):
         s.step(a.steps)
         s.sync()
     ms = s.last_ms()
-    launches = s.last_launches()
+    return s, ms, s.last_launches(), clk.summary()
+
+
+def form_switches(w, precision):
+    from tsuner_b200.abi import make_switches
+    sw = w.sw
+    return make_switches(order=sw.order, wbc=sw.wbc, bedload=sw.bedload, suspension=sw.suspension,
+                         read_files=sw.read_files, bedload_law=sw.bedload_law, precision=precision,
+                         grass_ag=sw.grass_ag, eta0=sw.eta0)
+
+
+def run_ours(a, rank, world, local, dist):
+    import tsuner_b200 as T
+    w, desc = workload(a.workload)
+    n = w.ncells
+    prim = 1 if a.precision == "fp32" else 0
+    # ---- primary form, device-timed with inputs resident in HBM
+    s, ms, launches, clocks = timed_form(T, w, form_switches(w, prim), a, local, dist)
     ms_max = dist_max(dist, ms, local)
+    V_prim = s.state()
+    sums = s.sums() if prim == 1 else None
     # ---- end to end through the C ABI with host buffers
     barrier(dist, local)
     t0 = time.perf_counter()
@@ -211,39 +230,61 @@ def run_ours(a, rank, world, local, dist):
     s.reset()
     s.step(a.steps)
     Vout = s.state()
-    ext = s.extrema()
-    e2e_s = time.perf_counter() - t0
-    e2e_s = dist_max(dist, e2e_s, local)
+    s.extrema()
+    e2e_s = dist_max(dist, time.perf_counter() - t0, local)
     s.close()
     assert np.isfinite(Vout).all()
+    # ---- the other form on the same workload and step count (rate + error)
+    other = None
+    if prim == 1 and not a.no_fp64:
+        s64, ms64, _, _ = timed_form(T, w, form_switches(w, 0), a, local, dist)
+        ms64 = dist_max(dist, ms64, local)
+        V64 = s64.state()
+        s64.close()
+        wet = V64[0] > w.p.epsilon_h
+        dh = V_prim[0] - V64[0]
+        m64 = float(V64[0].sum())
+        other = {"fp64_plain": {"value": round(world * n * a.steps / (ms64 / 1e3) / 1e6, 3),
+                                "unit": "Mcell-steps/s", "ms_per_step": round(ms64 / a.steps, 4)},
+                 "fp32_vs_fp64": {"steps": a.warmup + a.steps,
+                                  "linf_depth_m": float(np.abs(dh).max()),
+                                  "l2_depth_m": float(np.sqrt(np.mean(dh[wet] ** 2))) if wet.any() else 0.0,
+                                  "linf_qx": float(np.abs(V_prim[1] - V64[1]).max()),
+                                  "mass_drift_rel": (sums[0] - m64) / m64 if sums else None,
+                                  "speedup": round(ms64 / ms, 3)}}
     h2d = 5 * 8 * n + 4 * n + (w.CC.nbytes + w.tCC.nbytes if w.sw.read_files else 0)
     d2h = 5 * 8 * n + 3 * 8 * n
     if rank != 0:
         return None
     value = world * n * a.steps / (ms_max / 1e3) / 1e6
     hbm, kind = peaks()
-    bpc = BYTES_PER_CELL_STEP["f64"]
+    dtype = "f32" if prim == 1 else "f64"
+    bpc = BYTES_PER_CELL_STEP[dtype]
     achieved = bpc * n * a.steps / (ms / 1e3) / 1e9
-    tr = traffic_from_profiles("stage64_" + a.workload)
+    tr = traffic_from_profiles(("stage32_" if prim else "stage64_") + a.workload)
+    form = ("fp32 precision form (FP32 state, FP64 still-water level / wet-dry reconstruction / sums / time)"
+            if prim else "fp64 plain form (value-identical to the reference kernels)")
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mcell-steps/s", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 4),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
         "data": "synthetic (seeded generators, no dataset)",
-        "config": {"workload": desc, "form": "fp64 plain (one fused kernel per RK stage)",
-                   "cells": n, "l2": "state %.0f MB > 126 MB L2, no flush needed" % (5 * 8 * n / 1e6),
+        "config": {"workload": desc, "form": form + "; one fused kernel per RK stage",
+                   "cells": n, "l2": "state %.0f MB > 126 MB L2, no flush needed" % (5 * (4 if prim else 8) * n / 1e6),
                    "parallelism": "replicas x%d" % world},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "peak_kind": kind,
                      "bytes_per_cell_step": bpc,
                      "traffic": None if tr is None else round(tr[0] * n / 2.0, 0),
-                     "note": "FP64 plain form is FP64-pipe bound; algorithmic bytes over device time"},
+                     "note": "algorithmic bytes per cell-step x cells x steps / device time of the stage kernels"},
         "gpu_launches": launches,
         "e2e": {"value": round(world * n * a.steps / e2e_s / 1e6, 3), "unit": "Mcell-steps/s",
                 "h2d_bytes_per_step": int(h2d / a.steps), "d2h_bytes_per_step": int(d2h / a.steps),
                 "what": "tsu_set_state/mask/series + tsu_reset + tsu_step(K) + tsu_get_state/extrema, host buffers"},
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
+    if other:
+        line.update(other)
     if world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     return line
@@ -301,6 +342,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="nwave4096")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     rank, world, local, dist = dist_setup(a.gpus)

@@ -87,6 +87,9 @@ typedef struct TsuSwitches {
     int precision;    /* 0 = FP64 plain form (bitwise with the reference);
                          1 = FP32 precision form                              */
     double grass_ag;  /* A_g of the Grass law                               */
+    double eta0;      /* FP32 form: FP64 still-water level; the free surface is
+                         stored as the FP32 deviation eta - eta0 (use the
+                         sea level incl. sea-level rise)                      */
 } TsuSwitches;
 
 /* Per-run constants of the sediment laws, hoisted out of the per-cell code.
@@ -177,6 +180,9 @@ int tsu_sync(TsuSolver *s);
 int tsu_get_state(TsuSolver *s, double *V);
 int tsu_get_extrema(TsuSolver *s, double *hmax, double *bmin_rawH, double *eta_max);
 int tsu_get_time(TsuSolver *s, double *t, double *dt, long *steps);
+/* FP32 form only: FP64 sums over the grid after the last step of
+ * h (water volume / cell area) and of H + hc (bed + suspended sediment). */
+int tsu_get_sums(TsuSolver *s, double *water, double *sediment);
 int tsu_get_consts(TsuSolver *s, TsuConsts *k);
 /* Device timing of the last tsu_step() call in ms (CUDA events). */
 int tsu_last_step_ms(TsuSolver *s, double *ms);

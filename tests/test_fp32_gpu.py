@@ -1,0 +1,103 @@
+"""GPU tests of the FP32 precision form (TsuSwitches.precision = 1).
+
+It has no reference counterpart, so it is judged against the FP64 plain form
+(itself value-identical to the reference kernels):
+  * lake at rest is preserved exactly (z = eta - eta0 == 0, q == 0) over a
+    rough bed with a raised sea level -- the property FP32 loses without the
+    FP64 still-water level;
+  * with walls the FP64 water sum is conserved to FP32 round-off;
+  * the depth after a run stays within a stated L-inf bound of the FP64 form
+    (DEPTH_LINF_M), and the running extrema follow;
+  * every switch combination runs and stays finite and non-negative.
+"""
+import numpy as np
+import pytest
+
+import tsuner_b200 as T
+from tsuner_b200 import workloads as W
+from tsuner_b200.abi import make_switches
+
+pytestmark = pytest.mark.gpu
+
+DEPTH_LINF_M = 1e-3     # bound asserted here on the small cases
+MASS_REL = 1e-6
+
+
+def run(w, sw, nsteps):
+    s = T.Solver(w.p, sw)
+    s.set_state(w.V)
+    s.set_mask(w.mask)
+    if sw.read_files:
+        s.set_boundary_series(w.CC, w.tCC)
+    s.reset()
+    s.step(nsteps)
+    V = s.state()
+    ext = s.extrema()
+    t = s.time()
+    sums = s.sums() if sw.precision == 1 else None
+    s.close()
+    return V, ext, t, sums
+
+
+def sw_of(w, **kw):
+    d = dict(order=w.sw.order, wbc=w.sw.wbc, read_files=w.sw.read_files, eta0=w.sw.eta0)
+    d.update(kw)
+    return make_switches(**d)
+
+
+def test_lake_at_rest_is_exact_in_fp32():
+    w = W.nwave_shelf(160, 128, 20.0, slr=0.5, amp=0.0)
+    sw = sw_of(w, precision=1, read_files=0)
+    V, _, _, _ = run(w, sw, 200)
+    H32 = w.V[3].astype(np.float32).astype(np.float64)
+    assert np.array_equal(V[3], H32)
+    assert np.array_equal(V[0], np.maximum(0.5 + H32, 0.0))  # z == 0 exactly: h = eta0 + H
+    assert np.abs(V[1:3]).max() == 0.0
+    s = T.Solver(w.p, sw)
+    s.set_state(w.V)
+    s.set_mask(w.mask)
+    s.reset()
+    s.step(200)
+    ptr, pitch, plane, eb = s.device_state()
+    assert eb == 4
+    s.close()
+
+
+def test_water_conserved_with_walls_fp32():
+    w = W.hump(256, 192, 10.0, sigma=300.0)
+    sw = sw_of(w, precision=1)
+    s = T.Solver(w.p, sw)
+    s.set_state(w.V)
+    s.set_mask(w.mask)
+    s.reset()
+    s.step(1)
+    m1, _ = s.sums()
+    s.step(400)
+    m2, _ = s.sums()
+    s.close()
+    assert abs(m2 - m1) / m1 < MASS_REL, (m1, m2)
+
+
+@pytest.mark.parametrize("make,steps", [
+    (lambda: W.hump(256, 256, 10.0), 400),
+    (lambda: W.nwave_shelf(384, 256, 10.0, slr=0.5, amp=3.0, period=300.0, t_series=400.0), 400),
+])
+def test_depth_error_vs_fp64(make, steps):
+    w = make()
+    V64, e64, t64, _ = run(w, sw_of(w, precision=0), steps)
+    V32, e32, t32, _ = run(w, sw_of(w, precision=1), steps)
+    linf = np.abs(V32[0] - V64[0]).max()
+    assert linf <= DEPTH_LINF_M, linf
+    assert abs(t32[0] - t64[0]) / t64[0] < 1e-3
+    wet = (e64[0] > -1e29) & (e32[0] > -1e29)
+    assert np.abs(e32[0][wet] - e64[0][wet]).max() <= 10 * DEPTH_LINF_M
+
+
+@pytest.mark.parametrize("kw", [
+    dict(order=1), dict(wbc=0), dict(wbc=2), dict(bedload=0, suspension=0), dict(bedload_law=1),
+])
+def test_fp32_switch_variants_run(kw):
+    w = W.hump(96, 80, 10.0, sigma=150.0)
+    sw = sw_of(w, precision=1, **kw)
+    V, _, (t, dt, n), _ = run(w, sw, 100)
+    assert n == 100 and np.isfinite(V).all() and (V[0] >= 0).all()

@@ -1,0 +1,67 @@
+"""CPU: the oracle against golden fixtures produced by the reference's own
+CUDA kernels (tests/golden/make_golden.py, run on a B200).  This pins the
+oracle to the reference without a GPU: the outputs of the -nolto build must
+be reproduced value for value (state, running extrema, simulated time and
+next dt); the reference makefile recipe build (-dlto) within 1e-12 relative
+per field with identical wet/dry flags."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from tsuner_b200.abi import SimParams, TsuConsts, TsuSwitches
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FIXTURES = sorted(glob.glob(os.path.join(HERE, "*.npz")))
+PFIELDS = ["xmin", "xmax", "ymin", "ymax", "total_time", "save_time", "npx", "npy", "nvol", "CFL", "Q", "R",
+           "porosity", "DS", "FR", "Opar", "OC", "Dsg", "HQB", "vmax", "epsilon_h", "dx", "dy"]
+SFIELDS = ["order", "rk", "wbc", "bedload", "suspension", "read_files", "bedload_law", "precision", "grass_ag"]
+KFIELDS = ["vs", "Rp", "A_er", "sqrt_FR", "VP", "K_dep", "sqrt_OC", "DS5"]
+
+
+def _struct(cls, fields, vals):
+    s = cls()
+    for f, v in zip(fields, vals):
+        t = dict(cls._fields_)[f]
+        setattr(s, f, int(v) if t.__name__ in ("c_int", "c_long") else float(v))
+    return s
+
+
+def test_fixtures_present():
+    assert len(FIXTURES) >= 6, "golden fixtures missing (tests/golden/make_golden.py)"
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p)[:-4] for p in FIXTURES])
+def test_oracle_reproduces_reference_build(path):
+    d = np.load(path)
+    p = _struct(SimParams, PFIELDS, d["params"])
+    sw = _struct(TsuSwitches, SFIELDS, d["switches"])
+    k = _struct(TsuConsts, KFIELDS, d["consts"])
+    CC = d["CC"] if d["CC"].size else None
+    tCC = d["tCC"] if d["tCC"].size else None
+    r = oracle.OracleRun(p, sw, d["V_in"], d["mask"], CC, tCC, kconsts=k)
+    r.run(int(d["steps"]))
+    shp = (p.npy, p.npx)
+    assert np.array_equal(r.V, d["V_out"])
+    assert np.array_equal(r.hmax.reshape(shp), d["hmax"])
+    assert np.array_equal(r.bmin.reshape(shp), d["bmin"])
+    assert np.array_equal(r.eta_max.reshape(shp), d["eta_max"])
+    assert r.t.value == float(d["t"]) and r.dt.value == float(d["dt"])
+    rec = d["V_out_recipe"]
+    assert np.array_equal(r.V[0] > p.epsilon_h, rec[0] > p.epsilon_h)
+    for f in range(5):
+        assert np.abs(r.V[f] - rec[f]).max() <= 1e-12 * max(np.abs(rec[f]).max(), 1e-300)
+    assert abs(r.t.value - float(d["t_recipe"])) <= 1e-12 * float(d["t_recipe"])
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p)[:-4] for p in FIXTURES])
+def test_libm_constants_close_to_device(path):
+    """libm pow() vs device pow(): the two per-run constants agree to a few ulp."""
+    d = np.load(path)
+    p = _struct(SimParams, PFIELDS, d["params"])
+    k = oracle.consts(p)
+    dev = dict(zip(KFIELDS, d["consts"]))
+    for f in KFIELDS:
+        assert abs(getattr(k, f) - dev[f]) <= 4 * np.spacing(abs(dev[f])), f

@@ -1,14 +1,18 @@
 """GPU parity: the fused sm_100a kernels (through the C ABI) against
   (a) the CPU oracle on small seeded cases, for every switch combination, and
-  (b) the reference's own CUDA build (oracle/_ref, its unmodified kernels
-      driven step by step) on the same inputs, up to the full 512^2 x 2000
-      step configuration and a 4096^2 slice of the shelf configuration.
+  (b) the reference's own CUDA kernels (oracle/_ref: unmodified, driven step
+      by step) on the same inputs, up to the full 512^2 x 2000 step
+      configuration and a 4096^2 slice of the shelf configuration, in two
+      builds: the reference makefile recipe (-O2 -fmad=false -rdc -dlto) and
+      the same without -dlto.
 
-The bar (stated per field after the run): max|new - ref| / max|ref| <= 1e-12,
-wet/dry flags (h > epsilon_h) identical, and the same number of steps and
-simulated time.  Because the FP64 form keeps the reference's operation order
-and is built with -fmad=false like the reference, the tests also assert that
-the fields are equal value for value (0 == -0).
+Bars, per field after the run:
+  * vs the oracle and vs the -nolto reference build: equal value for value
+    (0 == -0), same steps, t and next dt -- the FP64 form keeps the
+    reference's operation order and is built with -fmad=false;
+  * vs the reference recipe build: max|new - ref| / max|ref| <= 1e-12, wet/dry
+    flags (h > epsilon_h) identical, same step count.  Its link-time code
+    generation rounds differently in the last bits (measured <= 3.2e-15).
 """
 import numpy as np
 import pytest
@@ -57,18 +61,22 @@ def rel_err(a, b):
 
 
 def assert_parity(new, ref, eps_h, exact=True, extrema=True):
+    assert np.array_equal(new["V"][0] > eps_h, ref["V"][0] > eps_h), "wet/dry flags differ"
     for f, name in enumerate(FIELDS):
         e = rel_err(new["V"][f], ref["V"][f])
         assert e <= REL_TOL, "%s rel err %.3e" % (name, e)
         if exact:
             assert np.array_equal(new["V"][f], ref["V"][f]), "%s not value-identical (rel %.3e)" % (name, e)
-    assert np.array_equal(new["V"][0] > eps_h, ref["V"][0] > eps_h)
     if extrema:
         for k in ("hmax", "bmin", "eta_max"):
             assert rel_err(new[k], ref[k]) <= REL_TOL, k
             if exact:
                 assert np.array_equal(new[k], ref[k]), k
-    assert new["t"] == ref["t"] and new["dt"] == ref["dt"]
+    if exact:
+        assert new["t"] == ref["t"] and new["dt"] == ref["dt"]
+    else:
+        assert abs(new["t"] - ref["t"]) <= REL_TOL * abs(ref["t"])
+        assert abs(new["dt"] - ref["dt"]) <= REL_TOL * abs(ref["dt"])
 
 
 # ------------------------------------------------------------- vs the oracle
@@ -152,13 +160,18 @@ need_ref = pytest.mark.skipif(not oracle.ref_available("default"), reason="oracl
 
 
 def ref_vs_new(w, nsteps, variant, sw):
-    if not oracle.ref_available(variant):
+    """Product vs the reference recipe build and vs its -nolto twin."""
+    if not (oracle.ref_available(variant) and oracle.ref_available(variant + "-nolto")):
         pytest.skip("reference variant %s not built" % variant)
     CC, tCC = (w.CC, w.tCC) if sw.read_files else (None, None)
     if variant == "default" and not sw.read_files:
         CC, tCC = W.expired_series(w.p.npx, w.p.npy)  # Read_files==1 build: walls
-    ref = oracle.ref_run(variant, w.p, w.V, w.mask, CC, tCC, nsteps)
     new = run_product(w, nsteps, sw)
+    ref = oracle.ref_run(variant, w.p, w.V, w.mask, CC, tCC, nsteps)
+    pin = oracle.ref_run(variant + "-nolto", w.p, w.V, w.mask, CC, tCC, nsteps)
+    assert ref["steps"] == pin["steps"] == nsteps
+    assert_parity(new, pin, w.p.epsilon_h, exact=True)
+    assert_parity(new, ref, w.p.epsilon_h, exact=False)
     return new, ref
 
 
@@ -171,24 +184,20 @@ def test_reference_build_switches():
 def test_config1_full_vs_reference_build():
     """512^2, dx=10 m, hump over the noisy 2 % slope, walls, 2000 steps."""
     w = W.hump(512, 512, 10.0, steps=2000)
-    new, ref = ref_vs_new(w, 2000, "default", make_switches(order=2, wbc=1, read_files=0))
-    assert ref["steps"] == 2000
-    assert_parity(new, ref, w.p.epsilon_h)
+    ref_vs_new(w, 2000, "default", make_switches(order=2, wbc=1, read_files=0))
 
 
 @need_ref
 def test_nwave_vs_reference_build():
     w = W.nwave_shelf(160, 96, 25.0, slr=0.5, amp=3.0, period=300.0, t_series=300.0)
-    new, ref = ref_vs_new(w, 300, "default", w.sw)
-    assert_parity(new, ref, w.p.epsilon_h)
+    ref_vs_new(w, 300, "default", w.sw)
 
 
 @need_ref
 def test_config2_slice_4096_vs_reference_build():
     """Full-size 4096^2 shelf with the N-wave series and harbour mask, 40 steps."""
     w = W.nwave_shelf(4096, 4096, 5.0)
-    new, ref = ref_vs_new(w, 40, "default", w.sw)
-    assert_parity(new, ref, w.p.epsilon_h)
+    ref_vs_new(w, 40, "default", w.sw)
 
 
 @pytest.mark.parametrize("variant,sw", [
@@ -201,15 +210,17 @@ def test_config2_slice_4096_vs_reference_build():
 def test_switch_variants_vs_reference_build(variant, sw):
     w = W.nwave_shelf(72, 56, 40.0, slr=0.5, amp=2.0, period=300.0, t_series=300.0)
     w.sw = make_switches(**sw)
-    new, ref = ref_vs_new(w, 150, variant, w.sw)
-    assert_parity(new, ref, w.p.epsilon_h)
+    ref_vs_new(w, 150, variant, w.sw)
 
 
 @need_ref
 def test_oracle_pinned_by_reference_build():
-    """The oracle itself matches the reference CUDA build."""
+    """The oracle itself matches the reference kernels: value for value the
+    -nolto build, within 1e-12 the recipe build."""
     w = W.nwave_shelf(96, 80, 30.0, slr=0.5, amp=2.0, period=300.0, t_series=300.0)
-    ref = oracle.ref_run("default", w.p, w.V, w.mask, w.CC, w.tCC, 120)
     k = run_product(w, 0)["k"]
     orc = run_oracle(w, 120, k)
-    assert_parity(orc, ref, w.p.epsilon_h)
+    pin = oracle.ref_run("default-nolto", w.p, w.V, w.mask, w.CC, w.tCC, 120)
+    ref = oracle.ref_run("default", w.p, w.V, w.mask, w.CC, w.tCC, 120)
+    assert_parity(orc, pin, w.p.epsilon_h, exact=True)
+    assert_parity(orc, ref, w.p.epsilon_h, exact=False)

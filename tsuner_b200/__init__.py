@@ -28,7 +28,7 @@ EXPORTS = [
     "tsu_derive_params", "tsu_parse_data_dat",
     "tsu_create", "tsu_destroy", "tsu_set_state", "tsu_set_mask", "tsu_set_boundary_series",
     "tsu_reset", "tsu_step", "tsu_run_until", "tsu_sync", "tsu_get_state", "tsu_get_extrema",
-    "tsu_get_time", "tsu_get_consts", "tsu_last_step_ms", "tsu_last_step_launches",
+    "tsu_get_time", "tsu_get_sums", "tsu_get_consts", "tsu_last_step_ms", "tsu_last_step_launches",
     "tsu_state_device", "tsu_strerror", "tsu_last_error", "tsu_version", "tsu_struct_sizes",
 ]
 
@@ -69,6 +69,7 @@ def lib():
             "tsu_get_extrema": ([vp, vp, vp, vp], C.c_int),
             "tsu_get_time": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_long)], C.c_int),
             "tsu_get_consts": ([vp, C.POINTER(TsuConsts)], C.c_int),
+            "tsu_get_sums": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
             "tsu_last_step_ms": ([vp, C.POINTER(C.c_double)], C.c_int),
             "tsu_last_step_launches": ([vp, C.POINTER(C.c_long)], C.c_int),
             "tsu_state_device": ([vp, C.POINTER(vp), C.POINTER(C.c_long), C.POINTER(C.c_long),
@@ -167,6 +168,12 @@ class Solver:
         t, dt, n = C.c_double(), C.c_double(), C.c_long()
         _ck(lib().tsu_get_time(self._h, C.byref(t), C.byref(dt), C.byref(n)), "tsu_get_time")
         return t.value, dt.value, n.value
+
+    def sums(self):
+        """FP32 form: FP64 (sum of h, sum of H + hc) over the grid."""
+        a, b = C.c_double(), C.c_double()
+        _ck(lib().tsu_get_sums(self._h, C.byref(a), C.byref(b)), "tsu_get_sums")
+        return a.value, b.value
 
     def consts(self):
         k = TsuConsts()

@@ -25,6 +25,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 UNIT_FLAGS = {
     "stage64.cu": ["-fmad=false"],
     "solver.cu": ["-fmad=false"],
+    # FP32 precision form: single precision may contract and use the hardware
+    # approximations; its FP64 islands are unaffected by this flag.
+    "stage32.cu": ["-use_fast_math"],
 }
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC]
 

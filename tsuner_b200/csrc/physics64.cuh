@@ -9,6 +9,8 @@
 // velocities are evaluated once per cell instead of five times, and face
 // states / edge fluxes never leave shared memory.
 #pragma once
+#include <math_constants.h>
+
 #include <cfloat>
 #include <cstdint>
 
@@ -30,32 +32,74 @@ struct Phys64 {
     double grass_ag;
 };
 
+// IEEE quotient and square root with the zero cases answered directly:
+// (+-0)/b for finite non-zero b is a zero with the XOR of the signs, and
+// sqrt(+-0) = +-0.  Value-identical to `/` and sqrt(); still water and dry
+// land make such operands the common case of this scheme.
+__device__ __forceinline__ double ddiv(double a, double b) {
+    if (a == 0.0 && b != 0.0 && isfinite(b)) return (signbit(a) != signbit(b)) ? -0.0 : 0.0;
+    return a / b;
+}
+__device__ __forceinline__ double dsqrt(double x) { return (x == 0.0) ? x : sqrt(x); }
+// As ddiv, also answering a non-zero, non-NaN numerator over a zero divisor
+// (an infinity with the XOR of the signs).
+__device__ __forceinline__ double ddiv_inf(double a, double b) {
+    if (b == 0.0 && a != 0.0 && !isnan(a)) return (signbit(a) != signbit(b)) ? -CUDART_INF : CUDART_INF;
+    return ddiv(a, b);
+}
+
 // SGN (Sim_parameters.hxx:29)
 __device__ __forceinline__ int sgn(double x) { return (fabs(x) < kEpsilon) ? 0 : ((x) > 0) ? 1 : -1; }
 
-// u_calculator_double (GPU/SedFlux.cuh:39-49)
-__device__ __forceinline__ void velocity(double h, double qx, double qy, double &ux, double &uy) {
-    double u = qx / (h + kEpsilon) * (double)(h >= kEps);
-    double v = qy / (h + kEpsilon) * (double)(h >= kEps);
-    double modu = sqrt(u * u + v * v);
+// u_calculator_double (GPU/SedFlux.cuh:39-49).  `modb` receives the modulus
+// of the returned velocity exactly as bedload() recomputes it
+// (GPU/SedFlux.cuh:157): when no clamping happened it is the same expression
+// on the same operands, so it is reused instead of a second sqrt.
+// A dry state (h < EPS) gives u = (q / (h + EPSILON)) * 0, i.e. a zero with
+// the sign of q; that is produced directly when the operands are finite and
+// h + EPSILON > 0, which is value-identical and skips two divisions.
+__device__ __forceinline__ void velocity(double h, double qx, double qy, double &ux, double &uy, double &modb) {
+    double d = h + kEpsilon;
+    if (!(h >= kEps) && d > 0.0 && !isnan(qx) && !isnan(qy)) {
+        ux = copysign(0.0, qx);
+        uy = copysign(0.0, qy);
+        modb = 0.0;
+        return;
+    }
+    double u = ddiv(qx, d) * (double)(h >= kEps);
+    double v = ddiv(qy, d) * (double)(h >= kEps);
+    double modu = dsqrt(u * u + v * v);
     if (modu > kVmax) {
         u = u / modu * kVmax;
         v = v / modu * kVmax;
+        modb = dsqrt(u * u + v * v);
+    } else {
+        modb = modu;
     }
     ux = u;
     uy = v;
 }
+__device__ __forceinline__ void velocity(double h, double qx, double qy, double &ux, double &uy) {
+    double m;
+    velocity(h, qx, qy, ux, uy, m);
+}
 
-// avg, the van-Leer-type limiter (GPU/Reconstructor.cu:19-31)
+// avg, the van-Leer-type limiter (GPU/Reconstructor.cu:19-31).  When the
+// numerator is a (signed) zero -- slopes of opposite sign or a zero slope --
+// the quotient equals the numerator, so the division is skipped.
 __device__ __forceinline__ double limiter(double a, double b) {
     double aa = fabs(a), bb = fabs(b);
-    return ((aa + bb) > kEpsilon) ? (a * bb + b * aa) / (aa + bb) : 0.0;
+    double den = aa + bb;
+    if (!(den > kEpsilon)) return 0.0;
+    double num = a * bb + b * aa;
+    if (num == 0.0) return num;
+    return num / den;
 }
 
 // state_filter_double (GPU/SedFlux.cuh:118-132)
 __device__ __forceinline__ void positivity_filter(double &h, double &qx, double &qy, double &hc) {
     h = h * (double)(h > 0.0);
-    double c = hc / (h + kEpsilon);
+    double c = ddiv(hc, h + kEpsilon);
     c = c * (double)(c > 0.0);
     double ux, uy;
     velocity(h, qx, qy, ux, uy);
@@ -68,24 +112,32 @@ struct State5 {
     double h, qx, qy, H, hc;
 };
 
-// bedload (GPU/SedFlux.cuh:150-168), or the Grass law when selected.
-__device__ __forceinline__ double bedload_flux(const Phys64 &P, double h, double ux, double uy) {
-    double modu = sqrt(ux * ux + uy * uy);
-    if (P.bedload_law == 1) return -(P.grass_ag * ux * modu * modu / (1.0 - P.porosity));
+// bedload (GPU/SedFlux.cuh:150-168), or the Grass law when selected; modu
+// is |u| as bedload() computes it.  The Ashida-Michiue product
+// K1*Q*max(O-OC,0)*max(sqrt(O)-sqrt(OC),0)*(h>HQB)*(h>5DS) has the sign of
+// u (K1 = 17u/(|u|+eps), every other factor >= +0), so whenever one factor
+// vanishes it is a zero with the sign of u and the return value -qb is
+// -copysign(0, u): that case skips the division and the sqrt.
+__device__ __forceinline__ double bedload_flux(const Phys64 &P, double h, double ux, double modu) {
+    if (P.bedload_law == 1) return -ddiv(P.grass_ag * ux * modu * modu, 1.0 - P.porosity);
     double O = P.Opar * modu * modu;
-    double K1 = 17.0 * ux / (modu + kEpsilon);
-    double qb = K1 * P.Q * fmax(O - P.OC, 0.0) * fmax(sqrt(O) - P.k.sqrt_OC, 0.0) *
+    if (!isnan(O) && (O <= P.OC || h <= P.HQB || h <= P.k.DS5)) return -copysign(0.0, ux);
+    double K1 = ddiv(17.0 * ux, modu + kEpsilon);
+    double qb = K1 * P.Q * fmax(O - P.OC, 0.0) * fmax(dsqrt(O) - P.k.sqrt_OC, 0.0) *
                 (double)(h > P.HQB) * (double)(h > P.k.DS5);
     return -qb;
 }
 
-// Cflux (GPU/SedFlux.cuh:171-179)
-__device__ __forceinline__ void phys_flux(const Phys64 &P, double h, double ux, double uy, double hc,
-                                          int fixed, double F[5]) {
+// Cflux (GPU/SedFlux.cuh:171-179).  With the bedload switched off or a fixed
+// bed, F[3] = bedload * 0 is a zero with the sign of the bedload, i.e.
+// -copysign(0, u) (NaN when |u| is NaN); produced without evaluating it.
+__device__ __forceinline__ void phys_flux(const Phys64 &P, double h, double ux, double modu, double hc,
+                                          int fixed, double uy, double F[5]) {
     F[0] = h * ux;
     F[1] = F[0] * ux;
     F[2] = F[0] * uy;
-    F[3] = bedload_flux(P, h, ux, uy) * (double)fixed * (double)P.bedload;
+    if (fixed != 0 && P.bedload != 0) F[3] = bedload_flux(P, h, ux, modu) * (double)fixed * (double)P.bedload;
+    else F[3] = isnan(modu) ? modu : -copysign(0.0, ux);
     F[4] = hc * ux;
 }
 
@@ -100,11 +152,11 @@ __device__ __forceinline__ void edge_flux(const Phys64 &P, const State5 &a, cons
     double qly = a.qy * dnx - a.qx * dny;
     double qrx = b.qx * dnx + b.qy * dny;
     double qry = b.qy * dnx - b.qx * dny;
-    double u0x, u0y, u1x, u1y;
-    velocity(a.h, qlx, qly, u0x, u0y);
-    velocity(b.h, qrx, qry, u1x, u1y);
-    double c0 = a.hc / (a.h + kEpsilon);
-    double c1 = b.hc / (b.h + kEpsilon);
+    double u0x, u0y, u1x, u1y, m0, m1;
+    velocity(a.h, qlx, qly, u0x, u0y, m0);
+    velocity(b.h, qrx, qry, u1x, u1y, m1);
+    double c0 = ddiv(a.hc, a.h + kEpsilon);
+    double c1 = ddiv(b.hc, b.h + kEpsilon);
 
     // hydrostatic reconstruction (:37-40)
     double zmH = fmin(a.H, b.H);
@@ -116,23 +168,23 @@ __device__ __forceinline__ void edge_flux(const Phys64 &P, const State5 &a, cons
     double deta = h1 - h0;
 
     double F0[5], F1[5];
-    phys_flux(P, h0, u0x, u0y, hc0, fixed, F0);
-    phys_flux(P, h1, u1x, u1y, hc1, fixed, F1);
+    phys_flux(P, h0, u0x, m0, hc0, fixed, u0y, F0);
+    phys_flux(P, h1, u1x, m1, hc1, fixed, u1y, F1);
 
     // Roe average + wave-speed bounds (GPU/SedFlux.cuh:181-199)
     double hm = 0.5 * (h0 + h1);
-    double s0q = sqrt(h0), s1q = sqrt(h1);
-    double umx = (s0q * u0x + s1q * u1x) / (s0q + s1q);
-    double SL = u0x - sqrt(kG * h0);
-    double SR = u1x + sqrt(kG * h1);
-    double cm = sqrt(kG * hm);
+    double s0q = dsqrt(h0), s1q = dsqrt(h1);
+    double umx = ddiv(s0q * u0x + s1q * u1x, s0q + s1q);
+    double SL = u0x - dsqrt(kG * h0);
+    double SR = u1x + dsqrt(kG * h1);
+    double cm = dsqrt(kG * hm);
     SL = fmin(SL, umx - cm);
     SR = fmax(SR, umx + cm);
 
     double a0, a1;
     if (SR - SL > kEpsilon) {
-        a0 = (SR * fabs(SL) - SL * fabs(SR)) / (SR - SL);
-        a1 = (fabs(SR) - fabs(SL)) / (SR - SL);
+        a0 = ddiv(SR * fabs(SL) - SL * fabs(SR), SR - SL);
+        a1 = ddiv(fabs(SR) - fabs(SL), SR - SL);
     } else {
         a0 = fmax(fabs(SL), fabs(SR));
         a1 = 0.0;
@@ -150,7 +202,7 @@ __device__ __forceinline__ void edge_flux(const Phys64 &P, const State5 &a, cons
     double s0 = sgn(b.H - a.H);
     double s1 = sgn(df[3]);
     double s2 = sgn(a1);
-    if (fabs(s0) > kEpsilon) s1 = s1 / s0;
+    if (fabs(s0) > kEpsilon) s1 = s1 * s0;  // s0 is +-1: s1/s0 == s1*s0 exactly
     else s1 = 0.0;
     double vis[5];
 #pragma unroll
@@ -212,10 +264,10 @@ __device__ __forceinline__ void series_state(const double *__restrict__ CC, cons
 __device__ __forceinline__ double cfl_dt(const Phys64 &P, double h, double qx, double qy) {
     double ux, uy;
     velocity(h, qx, qy, ux, uy);
-    double cg = sqrt(kG * h);
+    double cg = dsqrt(kG * h);
     double lx = fabs(ux) + cg;
     double ly = fabs(uy) + cg;
-    return P.CFL * 0.5 * fmin(P.dx / lx, P.dy / ly);
+    return P.CFL * 0.5 * fmin(ddiv_inf(P.dx, lx), ddiv_inf(P.dy, ly));
 }
 
 }  // namespace tsu

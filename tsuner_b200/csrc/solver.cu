@@ -1,12 +1,15 @@
 // solver.cu -- TsuSolver: device buffers, stepping and the tsu_* C ABI.
 //
 // Device layout (HBM): each field is a plane of npy rows with a row pitch
-// rounded up to 32 elements (256 B for FP64), planes consecutive:
+// rounded up to 32 elements (256 B in FP64, 128 B in FP32), planes
+// consecutive:
 //   bufA  [5][npy][pitch]  U^n at step entry / U^{n+1} at exit
 //   bufB  [5][npy][pitch]  U* (intermediate RK stage)
 //   hmax, bmin, eta_max [npy][pitch], mask [npy][pitch] uint8
-// About 105 B per cell in FP64 (the reference allocates ~796 B per cell,
-// GPU/main_TSUNER.cu:57-91).
+// FP64 plain form (planes h, qx, qy, H, hc): ~105 B per cell.  FP32 form
+// (planes z = eta - eta0, H, qx, qy, hc): ~53 B per cell plus an FP64
+// staging area used only by uploads/downloads.  The reference allocates
+// ~796 B per cell (GPU/main_TSUNER.cu:57-91).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -18,6 +21,7 @@
 #include <vector>
 
 #include "solver.h"
+#include "stage32.h"
 #include "stage64.h"
 #include "tsuner_b200.h"
 
@@ -26,16 +30,16 @@ using namespace tsu;
 namespace {
 thread_local char g_err[512] = "";
 std::mutex g_defaults_mu;
-TsuSwitches g_defaults = {2, 1, 1, 1, 1, 1, 0, 0, 1e-3};
+TsuSwitches g_defaults = {2, 1, 1, 1, 1, 1, 0, 0, 1e-3, 0.0};
 
 int cuda_fail(cudaError_t e, const char *what) {
     snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
     return (e == cudaErrorMemoryAllocation) ? TSU_ERR_GPU_OOM : TSU_ERR_CUDA;
 }
-#define CK(call)                                              \
-    do {                                                      \
-        cudaError_t _e = (call);                              \
-        if (_e != cudaSuccess) return cuda_fail(_e, #call);   \
+#define CK(call)                                            \
+    do {                                                    \
+        cudaError_t _e = (call);                            \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call); \
     } while (0)
 
 __global__ void set_scal_kernel(double *scal, int i, double v) { scal[i] = v; }
@@ -51,13 +55,14 @@ static int validate(const SimParams *p, const TsuSwitches *sw) {
     if (sw->rk != 1) return TSU_ERR_INVALID;
     if (sw->wbc < 0 || sw->wbc > 2) return TSU_ERR_INVALID;
     if (sw->bedload_law < 0 || sw->bedload_law > 1) return TSU_ERR_INVALID;
-    if (sw->precision != 0) return TSU_ERR_INVALID;
+    if (sw->precision != 0 && sw->precision != 1) return TSU_ERR_INVALID;
+    if (!std::isfinite(sw->eta0)) return TSU_ERR_INVALID;
     return TSU_OK;
 }
 
 extern "C" int tsu_switches_default(TsuSwitches *sw) {
     if (!sw) return TSU_ERR_INVALID;
-    TsuSwitches d = {2, 1, 1, 1, 1, 1, 0, 0, 1e-3};
+    TsuSwitches d = {2, 1, 1, 1, 1, 1, 0, 0, 1e-3, 0.0};
     *sw = d;
     return TSU_OK;
 }
@@ -84,13 +89,13 @@ extern "C" int tsu_derive_params(SimParams *p, double friction_datdat) {
 }
 
 static void free_all(TsuSolver *s) {
-    if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
-    if (s->graph) cudaGraphDestroy(s->graph);
+    s->invalidate_graph();
     cudaFree(s->A);
     cudaFree(s->B);
     cudaFree(s->hmax);
     cudaFree(s->bmin);
     cudaFree(s->eta);
+    cudaFree(s->stage64);
     cudaFree(s->mask);
     cudaFree(s->CC);
     cudaFree(s->tCC);
@@ -101,6 +106,65 @@ static void free_all(TsuSolver *s) {
     if (s->e0) cudaEventDestroy(s->e0);
     if (s->e1) cudaEventDestroy(s->e1);
     if (s->st) cudaStreamDestroy(s->st);
+}
+
+static void fill_phys(TsuSolver *s) {
+    const SimParams *p = &s->p;
+    const TsuSwitches *sw = &s->sw;
+    Phys64 &P = s->phys;
+    P.FR = p->FR;
+    P.eps_h = p->epsilon_h;
+    P.Opar = p->Opar;
+    P.OC = p->OC;
+    P.Q = p->Q;
+    P.HQB = p->HQB;
+    P.porosity = p->porosity;
+    P.CFL = p->CFL;
+    P.dx = p->dx;
+    P.dy = p->dy;
+    P.inv_dx = 1.0 / p->dx;  // GPU/main_TSUNER.cu:43-44
+    P.inv_dy = 1.0 / p->dy;
+    P.k = s->hconsts;
+    P.npx = p->npx;
+    P.npy = p->npy;
+    P.order = sw->order;
+    P.wbc = sw->wbc;
+    P.bedload = sw->bedload;
+    P.suspension = sw->suspension;
+    P.read_files = sw->read_files;
+    P.bedload_law = sw->bedload_law;
+    P.grass_ag = sw->grass_ag;
+    Phys32 &Q = s->phys32;
+    Q.eta0 = sw->eta0;
+    Q.FR = (float)p->FR;
+    Q.eps_h = (float)p->epsilon_h;
+    Q.Opar = (float)p->Opar;
+    Q.OC = (float)p->OC;
+    Q.Q = (float)p->Q;
+    Q.HQB = (float)p->HQB;
+    Q.porosity = (float)p->porosity;
+    Q.CFL = (float)p->CFL;
+    Q.dx = (float)p->dx;
+    Q.dy = (float)p->dy;
+    Q.inv_dx = (float)(1.0 / p->dx);
+    Q.inv_dy = (float)(1.0 / p->dy);
+    Q.vs = (float)s->hconsts.vs;
+    Q.inv_vs = (float)(1.0 / s->hconsts.vs);
+    Q.A_er = (float)s->hconsts.A_er;
+    Q.sqrt_FR = (float)s->hconsts.sqrt_FR;
+    Q.VP = (float)s->hconsts.VP;
+    Q.K_dep = (float)s->hconsts.K_dep;
+    Q.sqrt_OC = (float)s->hconsts.sqrt_OC;
+    Q.DS5 = (float)s->hconsts.DS5;
+    Q.npx = p->npx;
+    Q.npy = p->npy;
+    Q.order = sw->order;
+    Q.wbc = sw->wbc;
+    Q.bedload = sw->bedload;
+    Q.suspension = sw->suspension;
+    Q.read_files = sw->read_files;
+    Q.bedload_law = sw->bedload_law;
+    Q.grass_ag = (float)sw->grass_ag;
 }
 
 extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches *sw, int device) {
@@ -125,11 +189,12 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
     s->p.nvol = p->npx * p->npy;
     s->sw = *sw;
     s->device = device;
+    s->fp32 = (sw->precision == 1);
     s->pitch = ((long long)p->npx + 31) / 32 * 32;
     s->plane = s->pitch * p->npy;
-    const size_t pl = (size_t)s->plane * sizeof(double);
+    const size_t pl = (size_t)s->plane * s->elem();
     cudaError_t e = cudaSuccess;
-#define AL(ptr, bytes)                                            \
+#define AL(ptr, bytes) \
     if (e == cudaSuccess) e = cudaMalloc((void **)&(ptr), (bytes));
     AL(s->A, 5 * pl);
     AL(s->B, 5 * pl);
@@ -139,18 +204,19 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
     AL(s->mask, (size_t)s->plane);
     AL(s->scal, SC_N * sizeof(double));
     s->npartials = partials_needed(p->npx, p->npy);
-    AL(s->partials, s->npartials * sizeof(double));
+    AL(s->partials, 3 * s->npartials * sizeof(double));
     AL(s->ticket, sizeof(unsigned));
     AL(s->dconsts, sizeof(TsuConsts));
 #undef AL
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&s->e0);
     if (e == cudaSuccess) e = cudaEventCreate(&s->e1);
-    if (e == cudaSuccess) e = stage64_prepare();
+    if (e == cudaSuccess) e = s->fp32 ? stage32_prepare() : stage64_prepare();
     if (e == cudaSuccess) e = cudaMemsetAsync(s->A, 0, 5 * pl, s->st);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->B, 0, 5 * pl, s->st);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->mask, 1, (size_t)s->plane, s->st);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->ticket, 0, sizeof(unsigned), s->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->scal, 0, SC_N * sizeof(double), s->st);
     if (e == cudaSuccess) e = consts_launch(s->p, s->dconsts, s->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&s->hconsts, s->dconsts, sizeof(TsuConsts), cudaMemcpyDeviceToHost, s->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
@@ -160,29 +226,7 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
         delete s;
         return r;
     }
-    Phys64 &P = s->phys;
-    P.FR = p->FR;
-    P.eps_h = p->epsilon_h;
-    P.Opar = p->Opar;
-    P.OC = p->OC;
-    P.Q = p->Q;
-    P.HQB = p->HQB;
-    P.porosity = p->porosity;
-    P.CFL = p->CFL;
-    P.dx = p->dx;
-    P.dy = p->dy;
-    P.inv_dx = 1.0 / p->dx;  // GPU/main_TSUNER.cu:43-44
-    P.inv_dy = 1.0 / p->dy;
-    P.k = s->hconsts;
-    P.npx = p->npx;
-    P.npy = p->npy;
-    P.order = sw->order;
-    P.wbc = sw->wbc;
-    P.bedload = sw->bedload;
-    P.suspension = sw->suspension;
-    P.read_files = sw->read_files;
-    P.bedload_law = sw->bedload_law;
-    P.grass_ag = sw->grass_ag;
+    fill_phys(s);
     *out = s;
     return TSU_OK;
 }
@@ -196,9 +240,9 @@ extern "C" int tsu_destroy(TsuSolver *s) {
     return TSU_OK;
 }
 
-static int upload_plane(TsuSolver *s, double *dst, const double *src) {
-    CK(cudaMemcpy2DAsync(dst, s->pitch * sizeof(double), src, s->p.npx * sizeof(double),
-                         s->p.npx * sizeof(double), s->p.npy, cudaMemcpyHostToDevice, s->st));
+// FP64 staging planes of the FP32 form (allocated on first use).
+static int staging(TsuSolver *s) {
+    if (!s->stage64) CK(cudaMalloc((void **)&s->stage64, 5 * (size_t)s->plane * sizeof(double)));
     return TSU_OK;
 }
 
@@ -206,16 +250,21 @@ extern "C" int tsu_set_state(TsuSolver *s, const double *h, const double *qx, co
                              const double *hc) {
     if (!s || !h || !qx || !qy || !H) return TSU_ERR_INVALID;
     CK(cudaSetDevice(s->device));
+    int r = s->fp32 ? staging(s) : TSU_OK;
+    if (r) return r;
+    double *base = s->fp32 ? s->stage64 : (double *)s->A;
     const double *src[5] = {h, qx, qy, H, hc};
     for (int f = 0; f < 5; f++) {
-        double *dst = s->A + f * s->plane;
+        double *dst = base + f * s->plane;
         if (src[f]) {
-            int r = upload_plane(s, dst, src[f]);
-            if (r) return r;
+            CK(cudaMemcpy2DAsync(dst, s->pitch * sizeof(double), src[f], s->p.npx * sizeof(double),
+                                 s->p.npx * sizeof(double), s->p.npy, cudaMemcpyHostToDevice, s->st));
         } else {
             CK(cudaMemsetAsync(dst, 0, (size_t)s->plane * sizeof(double), s->st));
         }
     }
+    if (s->fp32)
+        CK(to32_launch(s->stage64, s->pitch, s->plane, s->p.npx, s->p.npy, s->sw.eta0, (float *)s->A, s->st));
     CK(cudaStreamSynchronize(s->st));
     s->has_state = true;
     s->ready = false;
@@ -274,21 +323,41 @@ extern "C" int tsu_set_boundary_series(TsuSolver *s, const double *CC, const dou
 
 Stage64Args TsuSolver::args() const {
     Stage64Args a;
-    a.bufA = A;
-    a.bufB = B;
+    a.bufA = (double *)A;
+    a.bufB = (double *)B;
     a.mask = mask;
     a.CC = CC;
     a.tCC = tCC;
     a.timeCC = timeCC;
-    a.hmax = hmax;
-    a.bmin = bmin;
-    a.eta_max = eta;
+    a.hmax = (double *)hmax;
+    a.bmin = (double *)bmin;
+    a.eta_max = (double *)eta;
     a.scal = scal;
     a.partials = partials;
     a.ticket = ticket;
     a.pitch = pitch;
     a.plane = plane;
     a.phys = phys;
+    return a;
+}
+
+Stage32Args TsuSolver::args32() const {
+    Stage32Args a;
+    a.bufA = (float *)A;
+    a.bufB = (float *)B;
+    a.mask = mask;
+    a.CC = CC;
+    a.tCC = tCC;
+    a.timeCC = timeCC;
+    a.hmax = (float *)hmax;
+    a.bmin = (float *)bmin;
+    a.eta_max = (float *)eta;
+    a.scal = scal;
+    a.partials = partials;
+    a.ticket = ticket;
+    a.pitch = pitch;
+    a.plane = plane;
+    a.phys = phys32;
     return a;
 }
 
@@ -308,19 +377,34 @@ extern "C" int tsu_reset(TsuSolver *s) {
     CK(cudaSetDevice(s->device));
     double init[SC_N] = {0.0, -1.0, HUGE_VAL, 0.0, 0.0, 0.0, 0.0, 0.0};
     CK(cudaMemcpyAsync(s->scal, init, sizeof(init), cudaMemcpyHostToDevice, s->st));
-    CK(fill_launch(s->hmax, s->plane, -1e30, s->st));  // set_inicializacion*, GPU/Volume_kernel.cu:112-137
-    CK(fill_launch(s->bmin, s->plane, -1e30, s->st));
-    CK(fill_launch(s->eta, s->plane, -1e30, s->st));
-    CK(initial_dt_launch(s->A, s->pitch, s->plane, s->phys, s->partials, s->ticket, s->scal, s->st));
+    if (s->fp32) {
+        CK(fill32_launch((float *)s->hmax, s->plane, -1e30f, s->st));
+        CK(fill32_launch((float *)s->bmin, s->plane, -1e30f, s->st));
+        CK(fill32_launch((float *)s->eta, s->plane, -1e30f, s->st));
+        CK(initial_dt32_launch((const float *)s->A, s->pitch, s->plane, s->phys32, s->partials, s->ticket, s->scal,
+                               s->st));
+    } else {
+        CK(fill_launch((double *)s->hmax, s->plane, -1e30, s->st));  // GPU/Volume_kernel.cu:112-137
+        CK(fill_launch((double *)s->bmin, s->plane, -1e30, s->st));
+        CK(fill_launch((double *)s->eta, s->plane, -1e30, s->st));
+        CK(initial_dt_launch((const double *)s->A, s->pitch, s->plane, s->phys, s->partials, s->ticket, s->scal,
+                             s->st));
+    }
     CK(cudaStreamSynchronize(s->st));
     s->ready = true;
     return TSU_OK;
 }
 
 int TsuSolver::launch_steps(long n) {
-    Stage64Args a = args();
-    for (long i = 0; i < n; i++)
-        for (int k = 0; k < sw.order; k++) CK(stage64_launch(sw.order, k, a, st));
+    if (fp32) {
+        Stage32Args a = args32();
+        for (long i = 0; i < n; i++)
+            for (int k = 0; k < sw.order; k++) CK(stage32_launch(sw.order, k, a, st));
+    } else {
+        Stage64Args a = args();
+        for (long i = 0; i < n; i++)
+            for (int k = 0; k < sw.order; k++) CK(stage64_launch(sw.order, k, a, st));
+    }
     return TSU_OK;
 }
 
@@ -371,7 +455,8 @@ extern "C" int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *s
     }
     CK(cudaSetDevice(s->device));
     double sc[SC_N];
-    CK(cudaMemcpy(sc, s->scal, sizeof(sc), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(sc, s->scal, sizeof(sc), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
     const double steps0 = sc[SC_STEPS];
     set_scal_kernel<<<1, 1, 0, s->st>>>(s->scal, SC_TEND, t_end);
     CK(cudaGetLastError());
@@ -392,7 +477,7 @@ extern "C" int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *s
     return TSU_OK;
 }
 
-double *TsuSolver::current() const {
+void *TsuSolver::current() const {
     if (sw.order == 2) return A;
     double sc[SC_N];
     if (cudaMemcpy(sc, scal, sizeof(sc), cudaMemcpyDeviceToHost) != cudaSuccess) return A;
@@ -403,7 +488,15 @@ extern "C" int tsu_get_state(TsuSolver *s, double *V) {
     if (!s || !V) return TSU_ERR_INVALID;
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->st));
-    const double *cur = s->current();
+    const double *cur = (const double *)s->current();
+    if (s->fp32) {
+        int r = staging(s);
+        if (r) return r;
+        CK(to64_launch((const float *)s->current(), s->pitch, s->plane, s->p.npx, s->p.npy, s->sw.eta0, s->stage64,
+                       s->st));
+        CK(cudaStreamSynchronize(s->st));
+        cur = s->stage64;
+    }
     const size_t n = (size_t)s->p.npx * s->p.npy;
     for (int f = 0; f < 5; f++)
         CK(cudaMemcpy2D(V + f * n, s->p.npx * sizeof(double), cur + f * s->plane, s->pitch * sizeof(double),
@@ -415,12 +508,21 @@ extern "C" int tsu_get_extrema(TsuSolver *s, double *hmax, double *bmin, double 
     if (!s) return TSU_ERR_INVALID;
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->st));
-    double *src[3] = {s->hmax, s->bmin, s->eta};
+    void *src[3] = {s->hmax, s->bmin, s->eta};
     double *dst[3] = {hmax, bmin, eta_max};
-    for (int f = 0; f < 3; f++)
-        if (dst[f])
-            CK(cudaMemcpy2D(dst[f], s->p.npx * sizeof(double), src[f], s->pitch * sizeof(double),
-                            s->p.npx * sizeof(double), s->p.npy, cudaMemcpyDeviceToHost));
+    for (int f = 0; f < 3; f++) {
+        if (!dst[f]) continue;
+        const double *from = (const double *)src[f];
+        if (s->fp32) {
+            int r = staging(s);
+            if (r) return r;
+            CK(widen_launch((const float *)src[f], s->stage64, s->plane, s->st));
+            CK(cudaStreamSynchronize(s->st));
+            from = s->stage64;
+        }
+        CK(cudaMemcpy2D(dst[f], s->p.npx * sizeof(double), from, s->pitch * sizeof(double), s->p.npx * sizeof(double),
+                        s->p.npy, cudaMemcpyDeviceToHost));
+    }
     return TSU_OK;
 }
 
@@ -433,6 +535,17 @@ extern "C" int tsu_get_time(TsuSolver *s, double *t, double *dt, long *steps) {
     if (t) *t = sc[SC_T];
     if (dt) *dt = sc[SC_DT];
     if (steps) *steps = (long)sc[SC_STEPS];
+    return TSU_OK;
+}
+
+extern "C" int tsu_get_sums(TsuSolver *s, double *water, double *sediment) {
+    if (!s || !s->fp32) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->st));
+    double sc[SC_N];
+    CK(cudaMemcpy(sc, s->scal, sizeof(sc), cudaMemcpyDeviceToHost));
+    if (water) *water = sc[SC_MASS];
+    if (sediment) *sediment = sc[SC_SED];
     return TSU_OK;
 }
 
@@ -465,7 +578,7 @@ extern "C" int tsu_state_device(TsuSolver *s, void **ptr, long *pitch_elems, lon
     if (ptr) *ptr = s->current();
     if (pitch_elems) *pitch_elems = (long)s->pitch;
     if (plane_elems) *plane_elems = (long)s->plane;
-    if (elem_bytes) *elem_bytes = 8;
+    if (elem_bytes) *elem_bytes = (int)s->elem();
     return TSU_OK;
 }
 
@@ -493,7 +606,7 @@ extern "C" int tsu_struct_sizes(size_t out[3]) {
     return TSU_OK;
 }
 
-extern "C" const char *tsu_version(void) { return "tsuner_b200 0.1 (sm_100a)"; }
+extern "C" const char *tsu_version(void) { return "tsuner_b200 0.2 (sm_100a)"; }
 
 // GPU/CheckCUDASupport.cu:21-44 contract: 0 ok, 1 no GPU, 2 no CUDA GPU, 3 bad index.
 extern "C" int checkCUDAsupport(int cudaDevice) {

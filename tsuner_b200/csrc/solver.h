@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "stage32.h"
 #include "stage64.h"
 #include "tsuner_b200.h"
 
@@ -11,10 +12,13 @@ struct TsuSolver {
     SimParams p{};
     TsuSwitches sw{};
     int device = 0;
+    bool fp32 = false;
     cudaStream_t st = nullptr;
     long long pitch = 0, plane = 0;  // elements
-    double *A = nullptr, *B = nullptr;
-    double *hmax = nullptr, *bmin = nullptr, *eta = nullptr;
+    // FP64 plain form: planes h, qx, qy, H, hc.  FP32 form: z, H, qx, qy, hc.
+    void *A = nullptr, *B = nullptr;
+    void *hmax = nullptr, *bmin = nullptr, *eta = nullptr;
+    double *stage64 = nullptr;  // FP32 form: FP64 staging planes for upload/download
     unsigned char *mask = nullptr;
     double *CC = nullptr, *tCC = nullptr;
     unsigned long timeCC = 0;
@@ -24,6 +28,7 @@ struct TsuSolver {
     TsuConsts *dconsts = nullptr;
     TsuConsts hconsts{};
     tsu::Phys64 phys{};
+    tsu::Phys32 phys32{};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -31,9 +36,11 @@ struct TsuSolver {
     bool has_state = false, ready = false, timed = false;
 
     tsu::Stage64Args args() const;
+    tsu::Stage32Args args32() const;
     int launch_steps(long n);
     void invalidate_graph();
-    double *current() const;
+    void *current() const;
+    size_t elem() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
 
 const char *tsu_last_error_detail();

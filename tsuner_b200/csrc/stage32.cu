@@ -1,0 +1,643 @@
+// stage32.cu -- FP32 precision form: one fused kernel per RK stage.
+//
+// Same pipeline as stage64.cu (tile + 2-cell halo in shared memory, faces,
+// each edge once, cell update, on-device dt/extrema), on the FP32 state
+// planes (z = eta - eta0, qx, qy, H, hc) with the FP64 islands of
+// physics32.cuh.  The last stage also accumulates the FP64 global sums of
+// water volume sum(h) and sediment volume sum(H + hc) (per-CTA partials,
+// reduced by the last CTA in a fixed order, so the sums are deterministic).
+// Algorithmic bytes per cell-step: 5 planes x 4 B read+write per stage
+// (stage 2 also reads U^n) = 100 B, mask 2 B, extrema 3 x 8 B = 126 B.
+#include <cuda_runtime.h>
+
+#include "physics32.cuh"
+#include "stage32.h"
+
+namespace tsu {
+
+namespace {
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+constexpr int LX = TX + 4, LY = TY + 4, PS = LX * LY;
+constexpr int FXW = TX + 2, FYH = TY + 2;
+// per loaded cell: z, H, qx, qy, hc (loaded) + h, ux, uy, c (derived)
+constexpr int kSV = 9 * PS;
+constexpr int kFlux = 20 * TY * TX;
+constexpr int kRegA = kSV > kFlux ? kSV : kFlux;
+constexpr int kFx = 12 * TY * FXW, kFy = 12 * FYH * TX;  // 2 faces x 6 floats
+constexpr int kDeta = 2 * TY * TX;
+constexpr int kFloats = kRegA + kFx + kFy + kDeta;
+constexpr int kWarps = NT / 32;
+}  // namespace
+
+size_t stage32_smem_bytes() { return sizeof(float) * kFloats + sizeof(double) * 3 * kWarps + PS + 64; }
+
+__device__ __forceinline__ int wrap_clamp32(int g, int n, bool periodic) {
+    if (periodic) {
+        g %= n;
+        return g < 0 ? g + n : g;
+    }
+    return g < 0 ? 0 : (g >= n ? n - 1 : g);
+}
+
+__device__ __forceinline__ void put_face(float *base, int stride, const Face32 &f) {
+    base[0] = f.h;
+    base[stride] = f.z;
+    base[2 * stride] = f.qx;
+    base[3 * stride] = f.qy;
+    base[4 * stride] = f.H;
+    base[5 * stride] = f.hc;
+}
+__device__ __forceinline__ Face32 get_face(const float *base, int stride) {
+    Face32 f;
+    f.h = base[0];
+    f.z = base[stride];
+    f.qx = base[2 * stride];
+    f.qy = base[3 * stride];
+    f.H = base[4 * stride];
+    f.hc = base[5 * stride];
+    return f;
+}
+
+// smem cell planes: 0 z, 1 H, 2 qx, 3 qy, 4 hc, 5 h, 6 ux, 7 uy, 8 c
+__device__ __forceinline__ void recon32(const Phys32 &P, const float *s, int c, int l, int r, Face32 &fm, Face32 &fp,
+                                        float &deta) {
+    const float hi = s[5 * PS + c], hl = s[5 * PS + l], hr = s[5 * PS + r];
+    const float zi = s[c], zl = s[l], zr = s[r];
+    const float Hi = s[PS + c], Hl = s[PS + l], Hr = s[PS + r];
+    float dh = limiter32(hi - hl, hr - hi);
+    if (0.5f * fabsf(dh) > hi) dh = copysignf(2.f * hi, dh);
+    // hydrostatic eta slope in FP64 (GPU/Reconstructor.cu:157-162)
+    double K = P.eta0 + (double)fminf(Hl, Hi);
+    float dl = (float)(fmax((double)zi + K, 0.0) - fmax((double)zl + K, 0.0));
+    K = P.eta0 + (double)fminf(Hr, Hi);
+    float dr = (float)(fmax((double)zr + K, 0.0) - fmax((double)zi + K, 0.0));
+    deta = limiter32(dl, dr);
+    const float dz = dh - deta;
+    fm.h = hi - 0.5f * dh;
+    fp.h = hi + 0.5f * dh;
+    fm.H = Hi - 0.5f * dz;
+    fp.H = Hi + 0.5f * dz;
+    fm.z = zi - 0.5f * deta;
+    fp.z = zi + 0.5f * deta;
+    const float uix = s[6 * PS + c], uiy = s[7 * PS + c];
+    float du = limiter32(uix - s[6 * PS + l], s[6 * PS + r] - uix);
+    float dq = hi * du + uix * dh;
+    fm.qx = s[2 * PS + c] - 0.5f * dq;
+    fp.qx = s[2 * PS + c] + 0.5f * dq;
+    du = limiter32(uiy - s[7 * PS + l], s[7 * PS + r] - uiy);
+    dq = hi * du + uiy * dh;
+    fm.qy = s[3 * PS + c] - 0.5f * dq;
+    fp.qy = s[3 * PS + c] + 0.5f * dq;
+    const float ci = s[8 * PS + c];
+    du = limiter32(ci - s[8 * PS + l], s[8 * PS + r] - ci);
+    fm.hc = (ci - 0.5f * du) * fm.h;
+    fp.hc = (ci + 0.5f * du) * fp.h;
+    filter32(fm, P.eta0);
+    filter32(fp, P.eta0);
+}
+
+template <int ORDER, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
+    extern __shared__ __align__(16) float smem32[];
+    const Phys32 &P = A.phys;
+    float *sV = smem32;
+    float *sFlux = smem32;
+    float *sFx = smem32 + kRegA;
+    float *sFy = sFx + kFx;
+    float *sDeta = sFy + kFy;
+    double *sRed = reinterpret_cast<double *>(sDeta + kDeta);  // [3][kWarps]
+    unsigned char *sM = reinterpret_cast<unsigned char *>(sRed + 3 * kWarps);
+    __shared__ int sLast;
+
+    const double t = A.scal[SC_T];
+    if (!(t < A.scal[SC_TEND])) return;
+    const double dtd = A.scal[SC_DT];
+    const float dt = (float)dtd;
+    const int npx = P.npx, npy = P.npy;
+    const bool periodic = (P.wbc == 2);
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const long long pitch = A.pitch, plane = A.plane;
+    const double eta0 = P.eta0;
+
+    const float *Vin;
+    const float *V0;
+    float *Vout;
+    int par = 0;
+    if (ORDER == 2) {
+        Vin = FIRST ? A.bufA : A.bufB;
+        V0 = A.bufA;
+        Vout = FIRST ? A.bufB : A.bufA;
+    } else {
+        par = (int)A.scal[SC_PAR];
+        Vin = par ? A.bufB : A.bufA;
+        V0 = Vin;
+        Vout = par ? A.bufA : A.bufB;
+    }
+
+    // ---- phase 1: load z, H, qx, qy, hc (+mask) with a 2-cell halo
+    for (int idx = tid; idx < PS; idx += NT) {
+        int ly = idx / LX, lx = idx - ly * LX;
+        int gx = wrap_clamp32(x0 + lx - 2, npx, periodic);
+        int gy = wrap_clamp32(y0 + ly - 2, npy, periodic);
+        long long g = (long long)gy * pitch + gx;
+#pragma unroll
+        for (int f = 0; f < 5; f++) sV[f * PS + idx] = Vin[f * plane + g];
+        sM[idx] = A.mask[g];
+    }
+    const int tx = tid % TX, ty = tid / TX;
+    const int gi = x0 + tx, gj = y0 + ty;
+    const bool own = (gi < npx) && (gj < npy);
+    const long long gown = (long long)(own ? gj : 0) * pitch + (own ? gi : 0);
+    float v0[5];
+    if (!FIRST) {
+#pragma unroll
+        for (int f = 0; f < 5; f++) v0[f] = V0[f * plane + gown];
+    }
+    __syncthreads();
+    const int cidx = (ty + 2) * LX + (tx + 2);
+    float vc[5];
+#pragma unroll
+    for (int f = 0; f < 5; f++) vc[f] = sV[f * PS + cidx];
+    if (FIRST) {
+#pragma unroll
+        for (int f = 0; f < 5; f++) v0[f] = vc[f];
+    }
+
+    // ---- phase 2: depth (FP64 island), velocity, concentration per cell
+    for (int idx = tid; idx < PS; idx += NT) {
+        const float h = (float)depth64(sV[idx], sV[PS + idx], eta0);
+        float ux, uy, m;
+        velocity32(h, sV[2 * PS + idx], sV[3 * PS + idx], ux, uy, m);
+        sV[5 * PS + idx] = h;
+        sV[6 * PS + idx] = ux;
+        sV[7 * PS + idx] = uy;
+        sV[8 * PS + idx] = (h > 0.f) ? fmaxf(sV[4 * PS + idx] * __frcp_rn(h), 0.f) : 0.f;
+    }
+    __syncthreads();
+    const float hcell = sV[5 * PS + cidx];
+
+    // ---- phase 3: faces
+    constexpr int NXI = FXW * TY, NYI = TX * FYH;
+    for (int item = tid; item < NXI + NYI; item += NT) {
+        int c, step, fstride, side, didx = -1;
+        float *dst;
+        if (item < NXI) {
+            int r = item / FXW, cx = item - r * FXW;
+            c = (r + 2) * LX + (cx + 1);
+            step = 1;
+            dst = sFx + r * FXW + cx;
+            fstride = TY * FXW;
+            side = 6 * TY * FXW;
+            int tc = cx - 1;
+            if (tc >= 0 && tc < TX) didx = r * TX + tc;
+        } else {
+            int it = item - NXI;
+            int ry = it / TX, cc = it - ry * TX;
+            c = (ry + 1) * LX + (cc + 2);
+            step = LX;
+            dst = sFy + ry * TX + cc;
+            fstride = FYH * TX;
+            side = 6 * FYH * TX;
+            int tr = ry - 1;
+            if (tr >= 0 && tr < TY) didx = TY * TX + tr * TX + cc;
+        }
+        Face32 fm, fp;
+        if (ORDER == 2) {
+            float deta;
+            recon32(P, sV, c, c - step, c + step, fm, fp, deta);
+            if (didx >= 0) sDeta[didx] = deta;
+        } else {
+            fm.h = sV[5 * PS + c];
+            fm.z = sV[c];
+            fm.H = sV[PS + c];
+            fm.qx = sV[2 * PS + c];
+            fm.qy = sV[3 * PS + c];
+            fm.hc = sV[4 * PS + c];
+            fp = fm;
+        }
+        put_face(dst, fstride, fm);
+        put_face(dst + side, fstride, fp);
+    }
+    __syncthreads();
+
+    // ---- phase 4: edges
+    const bool series_on = P.read_files && (t < A.tCC[A.timeCC - 2]);
+    constexpr int NV = (TX + 1) * TY, NH = TX * (TY + 1);
+    constexpr int FS = TY * TX;
+    for (int item = tid; item < NV + NH; item += NT) {
+        Face32 a, b;
+        int sgnn, fixed, seg = 0;
+        bool bnd = false, seam = false, vert;
+        float *outM = nullptr, *outP = nullptr;
+        if (item < NV) {
+            vert = true;
+            const int r = item / (TX + 1), e = item - r * (TX + 1);
+            const int ex = x0 + e, ey = y0 + r;
+            if (ey >= npy || ex > npx) continue;
+            const int ly = r + 2;
+            const float *Rf = sFx + (6 * TY + r) * FXW + e;
+            const float *Lf = sFx + r * FXW + (e + 1);
+            sgnn = 1;
+            if (periodic && (ex == 0 || ex == npx)) {
+                a = get_face(Rf, TY * FXW);
+                b = get_face(Lf, TY * FXW);
+                fixed = sM[ly * LX + e + 1];
+                seam = true;
+                seg = npx + ey;
+                if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
+                if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
+            } else if (ex == 0) {
+                a = get_face(Lf, TY * FXW);
+                sgnn = -1;
+                fixed = sM[ly * LX + e + 2];
+                bnd = true;
+                seg = 2 * npx + npy + ey;
+                outM = sFlux + 0 * 5 * FS + r * TX + e;
+            } else if (ex == npx) {
+                a = get_face(Rf, TY * FXW);
+                fixed = sM[ly * LX + e + 1];
+                bnd = true;
+                seg = npx + ey;
+                outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
+            } else {
+                a = get_face(Rf, TY * FXW);
+                b = get_face(Lf, TY * FXW);
+                fixed = (int)sM[ly * LX + e + 1] * (int)sM[ly * LX + e + 2];
+                if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
+                if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
+            }
+        } else {
+            vert = false;
+            const int it = item - NV;
+            const int e = it / TX, c = it - e * TX;
+            const int ex = x0 + c, ey = y0 + e;
+            if (ex >= npx || ey > npy) continue;
+            const float *Uf = sFy + (6 * FYH + e) * TX + c;
+            const float *Df = sFy + (e + 1) * TX + c;
+            sgnn = 1;
+            if (periodic && (ey == 0 || ey == npy)) {
+                a = get_face(Uf, FYH * TX);
+                b = get_face(Df, FYH * TX);
+                fixed = sM[(e + 1) * LX + c + 2];
+                seam = true;
+                seg = npx + npy + ex;
+                if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
+                if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
+            } else if (ey == 0) {
+                a = get_face(Df, FYH * TX);
+                sgnn = -1;
+                fixed = sM[(e + 2) * LX + c + 2];
+                bnd = true;
+                seg = ex;
+                outM = sFlux + 2 * 5 * FS + e * TX + c;
+            } else if (ey == npy) {
+                a = get_face(Uf, FYH * TX);
+                fixed = sM[(e + 1) * LX + c + 2];
+                bnd = true;
+                seg = npx + npy + ex;
+                outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
+            } else {
+                a = get_face(Uf, FYH * TX);
+                b = get_face(Df, FYH * TX);
+                fixed = (int)sM[(e + 1) * LX + c + 2] * (int)sM[(e + 2) * LX + c + 2];
+                if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
+                if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
+            }
+        }
+        if (bnd) {
+            b = a;
+            if (P.wbc == 1) {
+                if (vert) b.qx = -a.qx;
+                else b.qy = -a.qy;
+            }
+        }
+        if ((bnd || seam) && P.read_files) {
+            if (series_on) {  // GPU/VolumeSolver.cu:172-203 in FP64, then to the FP32 face
+                State5 g;
+                series_state(A.CC, A.tCC, t, npx, npy, seg, g);
+                b.H = (float)g.H;
+                b.h = (float)fmax(g.h, 0.0);
+                b.z = (g.h > 0.0) ? (float)(g.h - g.H - eta0) : dry_z(b.H, eta0);
+                b.qx = (float)g.qx;
+                b.qy = (float)g.qy;
+                b.hc = 0.f;
+            } else if (vert) {
+                b.qx = -a.qx;
+            } else {
+                b.qy = -a.qy;
+            }
+        }
+        // rotate to the edge normal: x edges n = (sgnn, 0), y edges n = (0, sgnn)
+        const float qna = vert ? sgnn * a.qx : sgnn * a.qy;
+        const float qta = vert ? sgnn * a.qy : -sgnn * a.qx;
+        const float qnb = vert ? sgnn * b.qx : sgnn * b.qy;
+        const float qtb = vert ? sgnn * b.qy : -sgnn * b.qx;
+        float Dm[5], Dp[5];
+        edge32(P, a, qna, qta, b, qnb, qtb, fixed, Dm, Dp);
+        // back to x/y: x edges (nx = sgnn, ny = 0), y edges (nx = 0, ny = sgnn)
+        float m1 = vert ? sgnn * Dm[1] : -sgnn * Dm[2];
+        float m2 = vert ? sgnn * Dm[2] : sgnn * Dm[1];
+        float p1 = vert ? sgnn * Dp[1] : -sgnn * Dp[2];
+        float p2 = vert ? sgnn * Dp[2] : sgnn * Dp[1];
+        if (outM) {
+            outM[0] = Dm[0];
+            outM[FS] = m1;
+            outM[2 * FS] = m2;
+            outM[3 * FS] = Dm[3];
+            outM[4 * FS] = Dm[4];
+        }
+        if (outP) {
+            outP[0] = Dp[0];
+            outP[FS] = p1;
+            outP[2 * FS] = p2;
+            outP[3 * FS] = Dp[3];
+            outP[4 * FS] = Dp[4];
+        }
+    }
+    __syncthreads();
+
+    // ---- phase 5: update (state: z, H, qx, qy, hc)
+    float dtcell = CUDART_INF_F;
+    double mass = 0.0, sed = 0.0;
+    if (own) {
+        float z = vc[0], H = vc[1], qx = vc[2], qy = vc[3], hc = vc[4];
+        if (ORDER == 2) {
+            qx -= dt * P.inv_dx * kGf * hcell * sDeta[ty * TX + tx];
+            qy -= dt * P.inv_dy * kGf * hcell * sDeta[TY * TX + ty * TX + tx];
+        }
+        {  // friction + erosion/deposition from U^n
+            const float h0 = (float)depth64(v0[0], v0[1], eta0);
+            float ux, uy, modu;
+            velocity32(h0, v0[2], v0[3], ux, uy, modu);
+            const float cf = (h0 > 0.f) ? dt * P.FR * modu * __frcp_rn(h0) : 0.f;
+            const float rf = __frcp_rn(1.f + cf);
+            qx *= rf;
+            qy *= rf;
+            const float c = (h0 + P.eps_h > 0.f) ? v0[4] * __frcp_rn(h0 + P.eps_h) : 0.f;
+            const float Z = P.A_er * modu * P.sqrt_FR * P.inv_vs;
+            const float Z5 = Z * Z * Z * Z * Z;
+            float Fe = P.VP * (1.3e-7f * Z5) * __frcp_rn(1.f + 4.3e-7f * Z5);
+            Fe = fminf(fmaxf(Fe, 0.f), 0.1f);
+            float Fd = fminf(fmaxf(P.vs * P.K_dep * c, 0.f), 0.1f);
+            const float phi = (Fe - Fd) * (float)P.suspension;
+            H -= dt * phi;
+            hc += dt * phi;
+            z += dt * phi;  // z = h - H - eta0 and H decreased by dt*phi
+        }
+        const float invx = dt * P.inv_dx, invy = dt * P.inv_dy;
+        const int cell = ty * TX + tx;
+        float dv[5];
+#pragma unroll
+        for (int f = 0; f < 5; f++)
+            dv[f] = invx * (sFlux[(0 * 5 + f) * FS + cell] + sFlux[(1 * 5 + f) * FS + cell]) +
+                    invy * (sFlux[(2 * 5 + f) * FS + cell] + sFlux[(3 * 5 + f) * FS + cell]);
+        z -= dv[0] - dv[3];
+        qx -= dv[1];
+        qy -= dv[2];
+        H -= dv[3];
+        hc -= dv[4];
+        if (ORDER == 2 && !FIRST) {  // RK2 average with U^n (linear in z)
+            z = 0.5f * (v0[0] + z);
+            H = 0.5f * (v0[1] + H);
+            qx = 0.5f * (v0[2] + qx);
+            qy = 0.5f * (v0[3] + qy);
+            hc = 0.5f * (v0[4] + hc);
+        }
+        const double hd = (double)z + eta0 + (double)H;
+        float h;
+        if (!(hd > 0.0)) {
+            h = 0.f;
+            z = dry_z(H, eta0);
+            qx = qy = hc = 0.f;
+        } else {
+            h = (float)hd;
+            float ux, uy, m;
+            velocity32(h, qx, qy, ux, uy, m);
+            const float c = fmaxf(hc * __frcp_rn(h), 0.f);
+            qx = h * ux;
+            qy = h * uy;
+            hc = h * c;
+        }
+        Vout[gown] = z;
+        Vout[plane + gown] = H;
+        Vout[2 * plane + gown] = qx;
+        Vout[3 * plane + gown] = qy;
+        Vout[4 * plane + gown] = hc;
+        if (LAST) {
+            if (h > P.eps_h) {
+                A.hmax[gown] = fmaxf(A.hmax[gown], h);
+                A.eta_max[gown] = fmaxf(A.eta_max[gown], (float)((double)z + eta0));
+            }
+            A.bmin[gown] = fmaxf(A.bmin[gown], H);
+            const float d = cfl_dt32(P, h, qx, qy);
+            if (!isnan(d)) dtcell = d;
+            mass = fmax(hd, 0.0);
+            sed = (double)H + (double)hc;
+        }
+    }
+
+    if (LAST) {
+        double m = (double)dtcell;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+            mass += __shfl_xor_sync(0xffffffffu, mass, o);
+            sed += __shfl_xor_sync(0xffffffffu, sed, o);
+        }
+        if ((tid & 31) == 0) {
+            sRed[tid >> 5] = m;
+            sRed[kWarps + (tid >> 5)] = mass;
+            sRed[2 * kWarps + (tid >> 5)] = sed;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double mm = sRed[0], ms = sRed[kWarps], sd = sRed[2 * kWarps];
+            for (int w = 1; w < kWarps; w++) {
+                mm = fmin(mm, sRed[w]);
+                ms += sRed[kWarps + w];
+                sd += sRed[2 * kWarps + w];
+            }
+            const unsigned nb = gridDim.x * gridDim.y;
+            const unsigned bI = blockIdx.y * gridDim.x + blockIdx.x;
+            A.partials[bI] = mm;
+            A.partials[nb + bI] = ms;
+            A.partials[2 * nb + bI] = sd;
+            __threadfence();
+            sLast = (atomicAdd(A.ticket, 1u) == nb - 1);
+        }
+        __syncthreads();
+        if (sLast) {
+            __threadfence();
+            const unsigned nb = gridDim.x * gridDim.y;
+            double mm = CUDART_INF;
+            for (unsigned i = tid; i < nb; i += NT) mm = fmin(mm, __ldcg(A.partials + i));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mm = fmin(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+            __syncthreads();
+            if ((tid & 31) == 0) sRed[tid >> 5] = mm;
+            __syncthreads();
+            if (tid == 0) {
+                for (int w = 0; w < kWarps; w++) mm = fmin(mm, sRed[w]);
+                // sums in a fixed order: deterministic FP64 totals
+                double ms = 0.0, sd = 0.0;
+                for (unsigned i = 0; i < nb; i++) {
+                    ms += __ldcg(A.partials + nb + i);
+                    sd += __ldcg(A.partials + 2 * nb + i);
+                }
+                A.scal[SC_T] = t + dtd;
+                A.scal[SC_DT] = finalize_dt(mm, (long long)npx * npy);
+                A.scal[SC_STEPS] += 1.0;
+                A.scal[SC_MASS] = ms;
+                A.scal[SC_SED] = sd;
+                if (ORDER == 1) A.scal[SC_PAR] = (double)(1 - par);
+                *A.ticket = 0u;
+                __threadfence();
+            }
+        }
+    }
+}
+
+// FP64 host planes (device copy) -> FP32 state; and back.
+__global__ void to32_kernel(const double *__restrict__ V64, long long pitch, long long plane, int npx, int npy,
+                            double eta0, float *__restrict__ V32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= npx || j >= npy) return;
+    const long long g = (long long)j * pitch + i;
+    const double h = V64[g], H = V64[3 * plane + g];
+    const float Hf = (float)H;
+    V32[plane + g] = Hf;
+    if (h > 0.0) {
+        V32[g] = (float)(h - (double)Hf - eta0);
+        V32[2 * plane + g] = (float)V64[plane + g];
+        V32[3 * plane + g] = (float)V64[2 * plane + g];
+        V32[4 * plane + g] = (float)V64[4 * plane + g];
+    } else {
+        V32[g] = dry_z(Hf, eta0);
+        V32[2 * plane + g] = 0.f;
+        V32[3 * plane + g] = 0.f;
+        V32[4 * plane + g] = 0.f;
+    }
+}
+
+__global__ void to64_kernel(const float *__restrict__ V32, long long pitch, long long plane, int npx, int npy,
+                            double eta0, double *__restrict__ V64) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= npx || j >= npy) return;
+    const long long g = (long long)j * pitch + i;
+    const float z = V32[g], H = V32[plane + g];
+    V64[g] = depth64(z, H, eta0);
+    V64[plane + g] = V32[2 * plane + g];
+    V64[2 * plane + g] = V32[3 * plane + g];
+    V64[3 * plane + g] = H;
+    V64[4 * plane + g] = V32[4 * plane + g];
+}
+
+__global__ void widen_kernel(const float *__restrict__ a, double *__restrict__ b, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = a[i];
+}
+
+__global__ void fill32_kernel(float *p, long long n, float v) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+// initial dt on the FP32 state, same finalisation as the reference reduction
+__global__ void __launch_bounds__(256) dt32_kernel(const float *__restrict__ V, long long pitch, long long plane,
+                                                   Phys32 P, double *partials, unsigned *ticket, double *scal) {
+    __shared__ double sRed[8];
+    __shared__ int sLast;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int gi = blockIdx.x * blockDim.x + threadIdx.x, gj = blockIdx.y * blockDim.y + threadIdx.y;
+    double m = CUDART_INF;
+    if (gi < P.npx && gj < P.npy) {
+        long long g = (long long)gj * pitch + gi;
+        float h = (float)depth64(V[g], V[plane + g], P.eta0);
+        float d = cfl_dt32(P, h, V[2 * plane + g], V[3 * plane + g]);
+        if (!isnan(d)) m = d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((tid & 31) == 0) sRed[tid >> 5] = m;
+    __syncthreads();
+    const unsigned nb = gridDim.x * gridDim.y;
+    if (tid == 0) {
+        for (int w = 1; w < 8; w++) m = fmin(m, sRed[w]);
+        partials[blockIdx.y * gridDim.x + blockIdx.x] = m;
+        __threadfence();
+        sLast = (atomicAdd(ticket, 1u) == nb - 1);
+    }
+    __syncthreads();
+    if (sLast) {
+        __threadfence();
+        double mm = CUDART_INF;
+        for (unsigned i = tid; i < nb; i += 256) mm = fmin(mm, __ldcg(partials + i));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mm = fmin(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+        __syncthreads();
+        if ((tid & 31) == 0) sRed[tid >> 5] = mm;
+        __syncthreads();
+        if (tid == 0) {
+            for (int w = 0; w < 8; w++) mm = fmin(mm, sRed[w]);
+            scal[SC_DT] = finalize_dt(mm, (long long)P.npx * P.npy);
+            *ticket = 0u;
+            __threadfence();
+        }
+    }
+}
+
+// ------------------------------------------------------------------ host side
+cudaError_t stage32_prepare() {
+    const int sm = (int)stage32_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(stage32_kernel<2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(stage32_kernel<2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(stage32_kernel<1, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    return e;
+}
+
+dim3 stage32_grid(int npx, int npy) { return dim3((npx + TX - 1) / TX, (npy + TY - 1) / TY); }
+
+cudaError_t stage32_launch(int order, int stage, const Stage32Args &a, cudaStream_t st) {
+    dim3 g = stage32_grid(a.phys.npx, a.phys.npy);
+    size_t sm = stage32_smem_bytes();
+    if (order == 2 && stage == 0) stage32_kernel<2, true, false><<<g, NT, sm, st>>>(a);
+    else if (order == 2) stage32_kernel<2, false, true><<<g, NT, sm, st>>>(a);
+    else stage32_kernel<1, true, true><<<g, NT, sm, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t to32_launch(const double *V64, long long pitch, long long plane, int npx, int npy, double eta0, float *V32,
+                        cudaStream_t st) {
+    dim3 b(256), g((npx + 255) / 256, npy);
+    to32_kernel<<<g, b, 0, st>>>(V64, pitch, plane, npx, npy, eta0, V32);
+    return cudaGetLastError();
+}
+
+cudaError_t to64_launch(const float *V32, long long pitch, long long plane, int npx, int npy, double eta0, double *V64,
+                        cudaStream_t st) {
+    dim3 b(256), g((npx + 255) / 256, npy);
+    to64_kernel<<<g, b, 0, st>>>(V32, pitch, plane, npx, npy, eta0, V64);
+    return cudaGetLastError();
+}
+
+cudaError_t widen_launch(const float *a, double *b, long long n, cudaStream_t st) {
+    widen_kernel<<<1184, 256, 0, st>>>(a, b, n);
+    return cudaGetLastError();
+}
+
+cudaError_t fill32_launch(float *p, long long n, float v, cudaStream_t st) {
+    fill32_kernel<<<1184, 256, 0, st>>>(p, n, v);
+    return cudaGetLastError();
+}
+
+cudaError_t initial_dt32_launch(const float *V, long long pitch, long long plane, const Phys32 &P, double *partials,
+                                unsigned *ticket, double *scal, cudaStream_t st) {
+    dim3 b(32, 8), g((P.npx + 31) / 32, (P.npy + 7) / 8);
+    dt32_kernel<<<g, b, 0, st>>>(V, pitch, plane, P, partials, ticket, scal);
+    return cudaGetLastError();
+}
+
+}  // namespace tsu

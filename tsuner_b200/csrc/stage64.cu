@@ -21,34 +21,30 @@
 //      minimum finished by the last CTA to arrive (no host round trip).
 // Face states and fluxes never touch global memory: per cell-step the
 // kernel moves the 250 algorithmic bytes instead of the reference's ~2 KB.
+// Phases 3 and 4 each have a single call site of the reconstruction and of
+// the Riemann solver (boundary cases only select operands), which keeps the
+// kernel body small enough for the instruction cache.
 #include <cuda_runtime.h>
+
+#include <cstdlib>
+#include <cstring>
 
 #include "physics64.cuh"
 #include "stage64.h"
 
 namespace tsu {
 
-namespace {
-
-constexpr int TX = S64_TX, TY = S64_TY, NT = TX * TY;
-constexpr int LX = TX + 4, LY = TY + 4;  // loaded tile with a 2-cell halo
-constexpr int FXW = TX + 2;              // x faces: tile columns -1..TX
-constexpr int FYH = TY + 2;              // y faces: tile rows -1..TY
-
-// shared-memory carve-up (doubles); region A (state + per-cell velocity) is
-// dead once the faces exist and is reused for the fluxes.
-constexpr int kSV = 5 * LY * LX;
-constexpr int kSUC = 3 * LY * LX;
-constexpr int kFlux = 4 * 5 * TY * TX;
-constexpr int kRegA = (kSV + kSUC) > kFlux ? (kSV + kSUC) : kFlux;
-constexpr int kFx = 2 * 5 * TY * FXW;
-constexpr int kFy = 2 * 5 * FYH * TX;
-constexpr int kDeta = 2 * TY * TX;
-constexpr int kDoubles = kRegA + kFx + kFy + kDeta;
-constexpr int kRed = NT / 32;
-}  // namespace
-
-size_t stage64_smem_bytes() { return sizeof(double) * (kDoubles + kRed) + LY * LX + 16; }
+template <int TX_, int TY_>
+struct Tile {
+    static constexpr int TX = TX_, TY = TY_, NT = TX * TY;
+    static constexpr int LX = TX + 4, LY = TY + 4, PS = LX * LY;  // loaded tile, 2-cell halo
+    static constexpr int FXW = TX + 2, FYH = TY + 2;               // faces incl. one halo cell
+    static constexpr int kSV = 5 * PS, kSUC = 3 * PS, kFlux = 20 * TY * TX;
+    static constexpr int kRegA = (kSV + kSUC) > kFlux ? (kSV + kSUC) : kFlux;
+    static constexpr int kFx = 10 * TY * FXW, kFy = 10 * FYH * TX, kDeta = 2 * TY * TX, kRed = NT / 32;
+    static constexpr int kDoubles = kRegA + kFx + kFy + kDeta + kRed;
+    static constexpr size_t smem() { return sizeof(double) * kDoubles + PS + 16; }
+};
 
 __device__ __forceinline__ int wrap_clamp(int g, int n, bool periodic) {
     if (periodic) {
@@ -60,11 +56,11 @@ __device__ __forceinline__ int wrap_clamp(int g, int n, bool periodic) {
 
 // MUSCL reconstruction of one cell along one direction, GPU/Reconstructor.cu
 // :124-194 (x) / :207-271 (y).  c/l/r index the centre and its two
-// neighbours in the smem tile.  Returns the two filtered faces (minus side,
-// plus side) and the hydrostatic slope deta.
+// neighbours in the smem tile (plane stride PS).  Returns the two filtered
+// faces (minus side, plus side) and the hydrostatic slope deta.
+template <int PS>
 __device__ __forceinline__ void reconstruct_dir(const double *sV, const double *sUC, int c, int l, int r,
-                                                bool xdir, State5 &fm, State5 &fp, double &deta) {
-    constexpr int PS = LY * LX;
+                                                State5 &fm, State5 &fp, double &deta) {
     const double hi = sV[c], Hi = sV[3 * PS + c];
     const double hl = sV[l], Hl = sV[3 * PS + l];
     const double hr = sV[r], Hr = sV[3 * PS + r];
@@ -110,7 +106,6 @@ __device__ __forceinline__ void reconstruct_dir(const double *sV, const double *
 
     positivity_filter(fm.h, fm.qx, fm.qy, fm.hc);
     positivity_filter(fp.h, fp.qx, fp.qy, fp.hc);
-    (void)xdir;
 }
 
 __device__ __forceinline__ void put5(double *base, int stride, const State5 &s) {
@@ -134,23 +129,25 @@ __device__ __forceinline__ void put5a(double *base, int stride, const double D[5
     for (int f = 0; f < 5; f++) base[f * stride] = D[f];
 }
 
-template <int ORDER, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(NT, 2) stage64_kernel(Stage64Args A) {
+template <int TX, int TY, int MINB, int ORDER, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(TX *TY, MINB) stage64_kernel(Stage64Args A) {
+    using T = Tile<TX, TY>;
+    constexpr int NT = T::NT, LX = T::LX, LY = T::LY, PS = T::PS, FXW = T::FXW, FYH = T::FYH;
     extern __shared__ __align__(16) double smem[];
     const Phys64 &P = A.phys;
-    double *sV = smem;                       // [5][LY][LX]
-    double *sUC = smem + kSV;                // [3][LY][LX]  (ux, uy, c)
-    double *sFlux = smem;                    // [4][5][TY][TX] aliases sV/sUC
-    double *sFx = smem + kRegA;              // [2][5][TY][FXW]
-    double *sFy = sFx + kFx;                 // [2][5][FYH][TX]
-    double *sDeta = sFy + kFy;               // [2][TY][TX]
-    double *sRed = sDeta + kDeta;            // [NT/32]
-    unsigned char *sM = reinterpret_cast<unsigned char *>(sRed + kRed);  // [LY][LX]
+    double *sV = smem;                  // [5][LY][LX]
+    double *sUC = smem + T::kSV;        // [3][LY][LX]  (ux, uy, c)
+    double *sFlux = smem;               // [4][5][TY][TX]  aliases sV/sUC (dead by then)
+    double *sFx = smem + T::kRegA;      // [2][5][TY][FXW]
+    double *sFy = sFx + T::kFx;         // [2][5][FYH][TX]
+    double *sDeta = sFy + T::kFy;       // [2][TY][TX]
+    double *sRed = sDeta + T::kDeta;    // [NT/32]
+    unsigned char *sM = reinterpret_cast<unsigned char *>(sRed + T::kRed);  // [LY][LX]
     __shared__ int sLast;
 
-    const double t = A.scal[0];
-    if (!(t < A.scal[2])) return;            // run_until predicate (uniform)
-    const double dt = A.scal[1];
+    const double t = A.scal[SC_T];
+    if (!(t < A.scal[SC_TEND])) return;  // run_until predicate (uniform)
+    const double dt = A.scal[SC_DT];
 
     const int npx = P.npx, npy = P.npy;
     const bool periodic = (P.wbc == 2);
@@ -158,7 +155,6 @@ __global__ void __launch_bounds__(NT, 2) stage64_kernel(Stage64Args A) {
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const long long pitch = A.pitch, plane = A.plane;
 
-    // buffers of this stage
     const double *Vin;
     const double *V0;
     double *Vout;
@@ -168,29 +164,28 @@ __global__ void __launch_bounds__(NT, 2) stage64_kernel(Stage64Args A) {
         V0 = A.bufA;
         Vout = FIRST ? A.bufB : A.bufA;
     } else {
-        par = (int)A.scal[4];
+        par = (int)A.scal[SC_PAR];
         Vin = par ? A.bufB : A.bufA;
         V0 = Vin;
         Vout = par ? A.bufA : A.bufB;
     }
 
     // ---- phase 1: tile + halo -> smem
-    for (int idx = tid; idx < LY * LX; idx += NT) {
+    for (int idx = tid; idx < PS; idx += NT) {
         int ly = idx / LX, lx = idx - ly * LX;
         int gx = wrap_clamp(x0 + lx - 2, npx, periodic);
         int gy = wrap_clamp(y0 + ly - 2, npy, periodic);
         long long g = (long long)gy * pitch + gx;
 #pragma unroll
-        for (int f = 0; f < 5; f++) sV[f * LY * LX + idx] = Vin[f * plane + g];
+        for (int f = 0; f < 5; f++) sV[f * PS + idx] = Vin[f * plane + g];
         sM[idx] = A.mask[g];
     }
     const int tx = tid % TX, ty = tid / TX;
     const int gi = x0 + tx, gj = y0 + ty;
     const bool own = (gi < npx) && (gj < npy);
     const long long gown = (long long)(own ? gj : 0) * pitch + (own ? gi : 0);
-    // U^n at the owned cell for friction / erosion / RK combine
     double v0[5];
-    if (!FIRST) {
+    if (!FIRST) {  // U^n of the owned cell (friction, erosion, RK combine)
 #pragma unroll
         for (int f = 0; f < 5; f++) v0[f] = V0[f * plane + gown];
     }
@@ -199,7 +194,7 @@ __global__ void __launch_bounds__(NT, 2) stage64_kernel(Stage64Args A) {
     const int cidx = (ty + 2) * LX + (tx + 2);
     double vc[5];
 #pragma unroll
-    for (int f = 0; f < 5; f++) vc[f] = sV[f * LY * LX + cidx];
+    for (int f = 0; f < 5; f++) vc[f] = sV[f * PS + cidx];
     if (FIRST) {
 #pragma unroll
         for (int f = 0; f < 5; f++) v0[f] = vc[f];
@@ -207,144 +202,160 @@ __global__ void __launch_bounds__(NT, 2) stage64_kernel(Stage64Args A) {
 
     // ---- phase 2: per-cell velocity and concentration
     if (ORDER == 2) {
-        for (int idx = tid; idx < LY * LX; idx += NT) {
+        for (int idx = tid; idx < PS; idx += NT) {
             double h = sV[idx];
             double ux, uy;
-            velocity(h, sV[LY * LX + idx], sV[2 * LY * LX + idx], ux, uy);
+            velocity(h, sV[PS + idx], sV[2 * PS + idx], ux, uy);
             sUC[idx] = ux;
-            sUC[LY * LX + idx] = uy;
-            sUC[2 * LY * LX + idx] = sV[4 * LY * LX + idx] / (h + kEpsilon);
+            sUC[PS + idx] = uy;
+            sUC[2 * PS + idx] = ddiv(sV[4 * PS + idx], h + kEpsilon);
         }
         __syncthreads();
     }
 
-    // ---- phase 3: faces
+    // ---- phase 3: faces (one reconstruction call site)
     constexpr int NXI = FXW * TY, NYI = TX * FYH;
     for (int item = tid; item < NXI + NYI; item += NT) {
-        State5 fm, fp;
-        double deta = 0.0;
+        int c, step, fstride, side, didx = -1;
+        double *dst;
         if (item < NXI) {
             int r = item / FXW, cx = item - r * FXW;  // tile col cx-1
-            int c = (r + 2) * LX + (cx + 1);
-            if (ORDER == 2) {
-                reconstruct_dir(sV, sUC, c, c - 1, c + 1, true, fm, fp, deta);
-                int tc = cx - 1;
-                if (tc >= 0 && tc < TX) sDeta[r * TX + tc] = deta;
-            } else {
-                fm = get5(sV + c, LY * LX);
-                fp = fm;
-            }
-            put5(sFx + (0 * 5 * TY + r) * FXW + cx, TY * FXW, fm);
-            put5(sFx + (1 * 5 * TY + r) * FXW + cx, TY * FXW, fp);
+            c = (r + 2) * LX + (cx + 1);
+            step = 1;
+            dst = sFx + r * FXW + cx;
+            fstride = TY * FXW;
+            side = 5 * TY * FXW;
+            int tc = cx - 1;
+            if (tc >= 0 && tc < TX) didx = r * TX + tc;
         } else {
             int it = item - NXI;
             int ry = it / TX, cc = it - ry * TX;  // tile row ry-1
-            int c = (ry + 1) * LX + (cc + 2);
-            if (ORDER == 2) {
-                reconstruct_dir(sV, sUC, c, c - LX, c + LX, false, fm, fp, deta);
-                int tr = ry - 1;
-                if (tr >= 0 && tr < TY) sDeta[TY * TX + tr * TX + cc] = deta;
-            } else {
-                fm = get5(sV + c, LY * LX);
-                fp = fm;
-            }
-            put5(sFy + (0 * 5 * FYH + ry) * TX + cc, FYH * TX, fm);
-            put5(sFy + (1 * 5 * FYH + ry) * TX + cc, FYH * TX, fp);
+            c = (ry + 1) * LX + (cc + 2);
+            step = LX;
+            dst = sFy + ry * TX + cc;
+            fstride = FYH * TX;
+            side = 5 * FYH * TX;
+            int tr = ry - 1;
+            if (tr >= 0 && tr < TY) didx = TY * TX + tr * TX + cc;
         }
+        State5 fm, fp;
+        if (ORDER == 2) {
+            double deta;
+            reconstruct_dir<PS>(sV, sUC, c, c - step, c + step, fm, fp, deta);
+            if (didx >= 0) sDeta[didx] = deta;
+        } else {  // first order: faces are the cell values (GPU/Reconstructor.cu:99-107)
+            fm = get5(sV + c, PS);
+            fp = fm;
+        }
+        put5(dst, fstride, fm);
+        put5(dst + side, fstride, fp);
     }
     __syncthreads();
 
-    // ---- phase 4: edges (each once per tile)
+    // ---- phase 4: edges (each once per tile, one Riemann call site)
     const bool series_on = P.read_files && (t < A.tCC[A.timeCC - 2]);
     constexpr int NV = (TX + 1) * TY, NH = TX * (TY + 1);
-    constexpr int FS = TY * TX;  // flux plane stride
+    constexpr int FS = TY * TX;  // flux plane stride; planes FL, FR, FD, FU
     for (int item = tid; item < NV + NH; item += NT) {
-        double Dm[5], Dp[5];
+        State5 a, b;
+        int nx, ny, fixed, seg = 0;
+        bool bnd = false, seam = false, vert;
+        double *outM = nullptr, *outP = nullptr;
         if (item < NV) {
-            int r = item / (TX + 1), e = item - r * (TX + 1);
-            int ex = x0 + e, ey = y0 + r;
+            vert = true;
+            const int r = item / (TX + 1), e = item - r * (TX + 1);
+            const int ex = x0 + e, ey = y0 + r;
             if (ey >= npy || ex > npx) continue;
             const int ly = r + 2;
-            // R face of tile col e-1 sits at sFx col e; L face of tile col e at col e+1
-            const double *Rf = sFx + (1 * 5 * TY + r) * FXW + e;
-            const double *Lf = sFx + (0 * 5 * TY + r) * FXW + (e + 1);
-            if (periodic && (ex == 0 || ex == npx)) {
-                State5 a = get5(Rf, TY * FXW), b = get5(Lf, TY * FXW);
-                if (P.read_files) {
-                    if (series_on) series_state(A.CC, A.tCC, t, npx, npy, npx + ey, b);
-                    else b.qx = -a.qx;
-                }
-                edge_flux(P, a, b, 1, 0, sM[ly * LX + e + 1], Dm, Dp);
-                if (e >= 1) put5a(sFlux + (1 * 5) * FS + r * TX + (e - 1), FS, Dm);
-                if (e < TX) put5a(sFlux + (0 * 5) * FS + r * TX + e, FS, Dp);
-            } else if (ex == 0) {
-                State5 a = get5(Lf, TY * FXW), b = a;
-                if (P.wbc == 1) b.qx = -a.qx;
-                if (P.read_files) {
-                    if (series_on) series_state(A.CC, A.tCC, t, npx, npy, 2 * npx + npy + ey, b);
-                    else b.qx = -a.qx;
-                }
-                edge_flux(P, a, b, -1, 0, sM[ly * LX + e + 2], Dm, Dp);
-                put5a(sFlux + (0 * 5) * FS + r * TX + e, FS, Dm);
-            } else if (ex == npx) {
-                State5 a = get5(Rf, TY * FXW), b = a;
-                if (P.wbc == 1) b.qx = -a.qx;
-                if (P.read_files) {
-                    if (series_on) series_state(A.CC, A.tCC, t, npx, npy, npx + ey, b);
-                    else b.qx = -a.qx;
-                }
-                edge_flux(P, a, b, 1, 0, sM[ly * LX + e + 1], Dm, Dp);
-                put5a(sFlux + (1 * 5) * FS + r * TX + (e - 1), FS, Dm);
-            } else {
-                State5 a = get5(Rf, TY * FXW), b = get5(Lf, TY * FXW);
-                int fixed = (int)sM[ly * LX + e + 1] * (int)sM[ly * LX + e + 2];
-                edge_flux(P, a, b, 1, 0, fixed, Dm, Dp);
-                if (e >= 1) put5a(sFlux + (1 * 5) * FS + r * TX + (e - 1), FS, Dm);
-                if (e < TX) put5a(sFlux + (0 * 5) * FS + r * TX + e, FS, Dp);
+            // R face of tile col e-1 is sFx col e; L face of tile col e is col e+1
+            const double *Rf = sFx + (5 * TY + r) * FXW + e;
+            const double *Lf = sFx + r * FXW + (e + 1);
+            nx = 1;
+            ny = 0;
+            if (periodic && (ex == 0 || ex == npx)) {  // seam: GPU/VolumeSolver.cu:262-275,289-298
+                a = get5(Rf, TY * FXW);
+                b = get5(Lf, TY * FXW);
+                fixed = sM[ly * LX + e + 1];
+                seam = true;
+                seg = npx + ey;
+                if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
+                if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
+            } else if (ex == 0) {  // west: GPU/VolumeSolver.cu:233-258
+                a = get5(Lf, TY * FXW);
+                nx = -1;
+                fixed = sM[ly * LX + e + 2];
+                bnd = true;
+                seg = 2 * npx + npy + ey;
+                outM = sFlux + 0 * 5 * FS + r * TX + e;
+            } else if (ex == npx) {  // east: GPU/VolumeSolver.cu:276-298
+                a = get5(Rf, TY * FXW);
+                fixed = sM[ly * LX + e + 1];
+                bnd = true;
+                seg = npx + ey;
+                outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
+            } else {  // interior: GPU/VolumeSolver.cu:300-314
+                a = get5(Rf, TY * FXW);
+                b = get5(Lf, TY * FXW);
+                fixed = (int)sM[ly * LX + e + 1] * (int)sM[ly * LX + e + 2];
+                if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
+                if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             }
         } else {
-            int it = item - NV;
-            int e = it / TX, c = it - e * TX;
-            int ex = x0 + c, ey = y0 + e;
+            vert = false;
+            const int it = item - NV;
+            const int e = it / TX, c = it - e * TX;
+            const int ex = x0 + c, ey = y0 + e;
             if (ex >= npx || ey > npy) continue;
-            // U face of tile row e-1 sits at sFy row e; D face of tile row e at row e+1
-            const double *Uf = sFy + (1 * 5 * FYH + e) * TX + c;
-            const double *Df = sFy + (0 * 5 * FYH + e + 1) * TX + c;
-            if (periodic && (ey == 0 || ey == npy)) {
-                State5 a = get5(Uf, FYH * TX), b = get5(Df, FYH * TX);
-                if (P.read_files) {
-                    if (series_on) series_state(A.CC, A.tCC, t, npx, npy, npx + npy + ex, b);
-                    else b.qy = -a.qy;
-                }
-                edge_flux(P, a, b, 0, 1, sM[(e + 1) * LX + c + 2], Dm, Dp);
-                if (e >= 1) put5a(sFlux + (3 * 5) * FS + (e - 1) * TX + c, FS, Dm);
-                if (e < TY) put5a(sFlux + (2 * 5) * FS + e * TX + c, FS, Dp);
-            } else if (ey == 0) {
-                State5 a = get5(Df, FYH * TX), b = a;
-                if (P.wbc == 1) b.qy = -a.qy;
-                if (P.read_files) {
-                    if (series_on) series_state(A.CC, A.tCC, t, npx, npy, ex, b);
-                    else b.qy = -a.qy;
-                }
-                edge_flux(P, a, b, 0, -1, sM[(e + 2) * LX + c + 2], Dm, Dp);
-                put5a(sFlux + (2 * 5) * FS + e * TX + c, FS, Dm);
-            } else if (ey == npy) {
-                State5 a = get5(Uf, FYH * TX), b = a;
-                if (P.wbc == 1) b.qy = -a.qy;
-                if (P.read_files) {
-                    if (series_on) series_state(A.CC, A.tCC, t, npx, npy, npx + npy + ex, b);
-                    else b.qy = -a.qy;
-                }
-                edge_flux(P, a, b, 0, 1, sM[(e + 1) * LX + c + 2], Dm, Dp);
-                put5a(sFlux + (3 * 5) * FS + (e - 1) * TX + c, FS, Dm);
-            } else {
-                State5 a = get5(Uf, FYH * TX), b = get5(Df, FYH * TX);
-                int fixed = (int)sM[(e + 1) * LX + c + 2] * (int)sM[(e + 2) * LX + c + 2];
-                edge_flux(P, a, b, 0, 1, fixed, Dm, Dp);
-                if (e >= 1) put5a(sFlux + (3 * 5) * FS + (e - 1) * TX + c, FS, Dm);
-                if (e < TY) put5a(sFlux + (2 * 5) * FS + e * TX + c, FS, Dp);
+            // U face of tile row e-1 is sFy row e; D face of tile row e is row e+1
+            const double *Uf = sFy + (5 * FYH + e) * TX + c;
+            const double *Df = sFy + (e + 1) * TX + c;
+            nx = 0;
+            ny = 1;
+            if (periodic && (ey == 0 || ey == npy)) {  // seam: GPU/VolumeSolver.cu:352-367,378-387
+                a = get5(Uf, FYH * TX);
+                b = get5(Df, FYH * TX);
+                fixed = sM[(e + 1) * LX + c + 2];
+                seam = true;
+                seg = npx + npy + ex;
+                if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
+                if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
+            } else if (ey == 0) {  // south: GPU/VolumeSolver.cu:324-349
+                a = get5(Df, FYH * TX);
+                ny = -1;
+                fixed = sM[(e + 2) * LX + c + 2];
+                bnd = true;
+                seg = ex;
+                outM = sFlux + 2 * 5 * FS + e * TX + c;
+            } else if (ey == npy) {  // north: GPU/VolumeSolver.cu:352-387
+                a = get5(Uf, FYH * TX);
+                fixed = sM[(e + 1) * LX + c + 2];
+                bnd = true;
+                seg = npx + npy + ex;
+                outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
+            } else {  // interior: GPU/VolumeSolver.cu:389-403
+                a = get5(Uf, FYH * TX);
+                b = get5(Df, FYH * TX);
+                fixed = (int)sM[(e + 1) * LX + c + 2] * (int)sM[(e + 2) * LX + c + 2];
+                if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
+                if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
             }
         }
+        if (bnd) {  // ghost = copy, wall mirror of the normal momentum
+            b = a;
+            if (P.wbc == 1) {
+                if (vert) b.qx = -a.qx;
+                else b.qy = -a.qy;
+            }
+        }
+        if ((bnd || seam) && P.read_files) {  // CC series while active, then wall
+            if (series_on) series_state(A.CC, A.tCC, t, npx, npy, seg, b);
+            else if (vert) b.qx = -a.qx;
+            else b.qy = -a.qy;
+        }
+        double Dm[5], Dp[5];
+        edge_flux(P, a, b, nx, ny, fixed, Dm, Dp);
+        if (outM) put5a(outM, FS, Dm);
+        if (outP) put5a(outP, FS, Dp);
     }
     __syncthreads();
 
@@ -354,8 +365,7 @@ __global__ void __launch_bounds__(NT, 2) stage64_kernel(Stage64Args A) {
         double vk[5];
 #pragma unroll
         for (int f = 0; f < 5; f++) vk[f] = vc[f];
-        if (ORDER == 2) {
-            // pressure source, GPU/Reconstructor.cu:197,274
+        if (ORDER == 2) {  // pressure source, GPU/Reconstructor.cu:197,274
             const double dtax = dt * P.inv_dx, dtay = dt * P.inv_dy;
             vk[1] -= dtax * kG * vc[0] * sDeta[ty * TX + tx];
             vk[2] -= dtay * kG * vc[0] * sDeta[TY * TX + ty * TX + tx];
@@ -365,14 +375,14 @@ __global__ void __launch_bounds__(NT, 2) stage64_kernel(Stage64Args A) {
         {
             double ux, uy;
             velocity(v0[0], v0[1], v0[2], ux, uy);
-            double modu = sqrt(ux * ux + uy * uy);
-            double cf = dt * P.FR * modu / (v0[0] + kEpsilon);
-            vk[1] /= (1.0 + cf);
-            vk[2] /= (1.0 + cf);
-            double c = v0[4] / (v0[0] + P.eps_h);
-            double Z = P.k.A_er * (modu * P.k.sqrt_FR) / P.k.vs;
+            double modu = dsqrt(ux * ux + uy * uy);
+            double cf = ddiv(dt * P.FR * modu, v0[0] + kEpsilon);
+            vk[1] = ddiv(vk[1], 1.0 + cf);
+            vk[2] = ddiv(vk[2], 1.0 + cf);
+            double c = ddiv(v0[4], v0[0] + P.eps_h);
+            double Z = ddiv(P.k.A_er * (modu * P.k.sqrt_FR), P.k.vs);
             double Z5 = Z * Z * Z * Z * Z;
-            double Es = (1.3e-7 * Z5) / (1 + 4.3e-7 * Z5);
+            double Es = ddiv(1.3e-7 * Z5, 1 + 4.3e-7 * Z5);
             double Fe = P.k.VP * Es;
             if (Fe > 0.1) Fe = 0.1;
             Fe = Fe * (double)(Fe > 0.0);
@@ -419,15 +429,16 @@ __global__ void __launch_bounds__(NT, 2) stage64_kernel(Stage64Args A) {
     }
 
     if (LAST) {
-        // CTA minimum with warp shuffles, then the last CTA finishes the
-        // global minimum and advances t (GPU/main_TSUNER.cu:185,190-192).
+        // CTA minimum with warp shuffles; the last CTA to finish reduces the
+        // partials, advances t and publishes the next dt
+        // (GPU/main_TSUNER.cu:185,190-192).
         double m = dtcell;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
         if ((tid & 31) == 0) sRed[tid >> 5] = m;
         __syncthreads();
         if (tid < 32) {
-            m = (tid < kRed) ? sRed[tid] : CUDART_INF;
+            m = (tid < T::kRed) ? sRed[tid] : CUDART_INF;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
             if (tid == 0) {
@@ -447,14 +458,15 @@ __global__ void __launch_bounds__(NT, 2) stage64_kernel(Stage64Args A) {
             for (unsigned i = tid; i < nb; i += NT) mm = fmin(mm, __ldcg(A.partials + i));
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) mm = fmin(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+            __syncthreads();
             if ((tid & 31) == 0) sRed[tid >> 5] = mm;
             __syncthreads();
             if (tid == 0) {
-                for (int w = 0; w < kRed; w++) mm = fmin(mm, sRed[w]);
-                A.scal[0] = t + dt;
-                A.scal[1] = finalize_dt(mm, (long long)npx * npy);
-                A.scal[3] += 1.0;
-                if (ORDER == 1) A.scal[4] = (double)(1 - par);
+                for (int w = 0; w < T::kRed; w++) mm = fmin(mm, sRed[w]);
+                A.scal[SC_T] = t + dt;
+                A.scal[SC_DT] = finalize_dt(mm, (long long)npx * npy);
+                A.scal[SC_STEPS] += 1.0;
+                if (ORDER == 1) A.scal[SC_PAR] = (double)(1 - par);
                 *A.ticket = 0u;
                 __threadfence();
             }
@@ -480,17 +492,26 @@ __global__ void __launch_bounds__(256) dt_partials_kernel(const double *__restri
     for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((tid & 31) == 0) sRed[tid >> 5] = m;
     __syncthreads();
+    const unsigned nb = gridDim.x * gridDim.y;
     if (tid == 0) {
         for (int w = 1; w < 8; w++) m = fmin(m, sRed[w]);
-        const unsigned nb = gridDim.x * gridDim.y;
         partials[blockIdx.y * gridDim.x + blockIdx.x] = m;
         __threadfence();
         sLast = (atomicAdd(ticket, 1u) == nb - 1);
-        if (sLast) {
-            __threadfence();
-            double mm = CUDART_INF;
-            for (unsigned i = 0; i < nb; i++) mm = fmin(mm, __ldcg(partials + i));
-            scal[1] = finalize_dt(mm, (long long)P.npx * P.npy);
+    }
+    __syncthreads();
+    if (sLast) {
+        __threadfence();
+        double mm = CUDART_INF;
+        for (unsigned i = tid; i < nb; i += 256) mm = fmin(mm, __ldcg(partials + i));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mm = fmin(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+        __syncthreads();
+        if ((tid & 31) == 0) sRed[tid >> 5] = mm;
+        __syncthreads();
+        if (tid == 0) {
+            for (int w = 0; w < 8; w++) mm = fmin(mm, sRed[w]);
+            scal[SC_DT] = finalize_dt(mm, (long long)P.npx * P.npy);
             *ticket = 0u;
             __threadfence();
         }
@@ -525,28 +546,61 @@ __global__ void consts_kernel(SimParams p, TsuConsts *k) {
 }
 
 // ------------------------------------------------------------------ host side
-#define S64_INSTANCE(O, F, L) \
-    template __global__ void stage64_kernel<O, F, L>(Stage64Args);
-S64_INSTANCE(2, true, false)
-S64_INSTANCE(2, false, true)
-S64_INSTANCE(1, true, true)
+namespace {
 
-cudaError_t stage64_prepare() {
-    size_t sm = stage64_smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(stage64_kernel<2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage64_kernel<2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(stage64_kernel<1, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    return e;
+struct Variant {
+    int tx, ty;
+    size_t smem;
+    void (*k[3])(Stage64Args);  // order2 stage0, order2 stage1, order1
+};
+
+template <int TX, int TY, int MINB>
+Variant make_variant() {
+    Variant v;
+    v.tx = TX;
+    v.ty = TY;
+    v.smem = Tile<TX, TY>::smem();
+    v.k[0] = stage64_kernel<TX, TY, MINB, 2, true, false>;
+    v.k[1] = stage64_kernel<TX, TY, MINB, 2, false, true>;
+    v.k[2] = stage64_kernel<TX, TY, MINB, 1, true, true>;
+    return v;
 }
 
-dim3 stage64_grid(int npx, int npy) { return dim3((npx + TX - 1) / TX, (npy + TY - 1) / TY); }
+const Variant &variant() {
+    static Variant v = [] {
+        const char *e = std::getenv("TSU_TILE64");
+        if (e && !std::strcmp(e, "16x16")) return make_variant<16, 16, 2>();
+        if (e && !std::strcmp(e, "32x16")) return make_variant<32, 16, 1>();
+        if (e && !std::strcmp(e, "16x8")) return make_variant<16, 8, 4>();
+        if (e && !std::strcmp(e, "32x4")) return make_variant<32, 4, 4>();
+        return make_variant<32, 8, 2>();
+    }();
+    return v;
+}
+
+}  // namespace
+
+size_t stage64_smem_bytes() { return variant().smem; }
+
+cudaError_t stage64_prepare() {
+    const Variant &v = variant();
+    for (int i = 0; i < 3; i++) {
+        cudaError_t e = cudaFuncSetAttribute(v.k[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+dim3 stage64_grid(int npx, int npy) {
+    const Variant &v = variant();
+    return dim3((npx + v.tx - 1) / v.tx, (npy + v.ty - 1) / v.ty);
+}
 
 cudaError_t stage64_launch(int order, int stage, const Stage64Args &a, cudaStream_t st) {
+    const Variant &v = variant();
     dim3 g = stage64_grid(a.phys.npx, a.phys.npy);
-    size_t sm = stage64_smem_bytes();
-    if (order == 2 && stage == 0) stage64_kernel<2, true, false><<<g, NT, sm, st>>>(a);
-    else if (order == 2) stage64_kernel<2, false, true><<<g, NT, sm, st>>>(a);
-    else stage64_kernel<1, true, true><<<g, NT, sm, st>>>(a);
+    int which = (order == 2) ? (stage == 0 ? 0 : 1) : 2;
+    v.k[which]<<<g, v.tx * v.ty, v.smem, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -568,8 +622,8 @@ cudaError_t consts_launch(const SimParams &p, TsuConsts *k, cudaStream_t st) {
 }
 
 size_t partials_needed(int npx, int npy) {
-    dim3 g = stage64_grid(npx, npy);
-    size_t a = (size_t)g.x * g.y;
+    // enough for every tile shape and for the 32x8 initial-dt grid
+    size_t a = (size_t)((npx + 15) / 16) * ((npy + 3) / 4);
     size_t b = (size_t)((npx + 31) / 32) * ((npy + 7) / 8);
     return a > b ? a : b;
 }

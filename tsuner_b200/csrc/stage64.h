@@ -18,7 +18,9 @@ namespace tsu {
 //   [0] simulated time t      [1] dt of the next step
 //   [2] t_end of run_until (steps execute only while t < t_end)
 //   [3] steps taken           [4] order-1 ping-pong parity
-enum { SC_T = 0, SC_DT = 1, SC_TEND = 2, SC_STEPS = 3, SC_PAR = 4, SC_N = 8 };
+//   [5] FP32 form: sum of water depth after the last step (FP64)
+//   [6] FP32 form: sum of H + hc after the last step (FP64)
+enum { SC_T = 0, SC_DT = 1, SC_TEND = 2, SC_STEPS = 3, SC_PAR = 4, SC_MASS = 5, SC_SED = 6, SC_N = 8 };
 
 struct Stage64Args {
     double *bufA;           // U^n at step entry (and U^{n+1} at exit, order 2)

@@ -174,7 +174,7 @@ def nwave_shelf(npx=4096, npy=4096, dx=5.0, steps=5000, seed=2, slr=0.5, amp=3.0
         t_series = 2000.0
     CC, tCC = boundary_series(H, slr, t_series, amp=amp, period=period)
     p = make_params(npx, npy, dx, dx)
-    sw = make_switches(order=2, wbc=1, read_files=1)
+    sw = make_switches(order=2, wbc=1, read_files=1, eta0=slr)
     return Workload("nwave%dx%d" % (npx, npy), p, sw, V, mask, CC, tCC, slr=slr, steps=steps)
 
 
@@ -197,5 +197,5 @@ def humps_shelf(npx=8192, npy=8192, dx=5.0, steps=2000, seed=3, slr=0.0, nhumps=
     V[0] = np.maximum(slr + eta + H, 0.0)
     V[3] = H
     p = make_params(npx, npy, dx, dx)
-    sw = make_switches(order=2, wbc=1, read_files=0)
+    sw = make_switches(order=2, wbc=1, read_files=0, eta0=slr)
     return Workload("humps%dx%d" % (npx, npy), p, sw, V, mask, slr=slr, steps=steps)
