@@ -17,6 +17,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 OBJ = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libtsuner_b200.so")
+EXE = os.path.join(PKG, "tsuner.exe")
 INC = os.path.join(ROOT, "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -73,6 +74,11 @@ def build(force=False, verbose=False):
                 sys.stdout.write(r.stderr)
     if force or _stale(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"])
+    # tsuner.exe front end, linked against the library (rpath = its folder)
+    app = os.path.join(PKG, "app", "tsuner_main.cpp")
+    if force or _stale(EXE, [app, LIB] + hdrs):
+        _run(["g++", "-O2", "-std=c++17", "-I" + INC, "-I/usr/local/cuda/include", app, "-o", EXE,
+              "-L" + PKG, "-ltsuner_b200", "-Wl,-rpath,$ORIGIN", "-L/usr/local/cuda/lib64", "-lcudart"])
     return LIB
 
 

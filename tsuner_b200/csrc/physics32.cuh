@@ -27,8 +27,13 @@ constexpr float kGf = 9.81f;
 constexpr float kEpsf = 1e-6f;   // velocity cutoff EPS (Sim_parameters.hxx:35)
 constexpr float kVmaxf = 10.0f;  // VMAX (Sim_parameters.hxx:36)
 
+// Depth margin above which an FP32 sum z + (eta0 + H) cannot change sign by
+// rounding (FP32 relative error ~6e-8 on |eta0 + H| < 1e5 m).
+constexpr float kWetMarginf = 1e-2f;
+
 struct Phys32 {
     double eta0;  // still-water level (FP64)
+    float eta0f;  // the same rounded to FP32 (only used beyond kWetMarginf)
     float FR, eps_h, Opar, OC, Q, HQB, porosity, CFL, dx, dy, inv_dx, inv_dy;
     float vs, A_er, sqrt_FR, VP, K_dep, sqrt_OC, DS5, inv_vs;
     int npx, npy;
@@ -113,11 +118,24 @@ __device__ __forceinline__ void edge32(const Phys32 &P, const Face32 &a, float q
     velocity32(b.h, qnb, qtb, u1, v1, m1);
     float c0 = (a.h > 0.f) ? a.hc * __frcp_rn(a.h) : 0.f;
     float c1 = (b.h > 0.f) ? b.hc * __frcp_rn(b.h) : 0.f;
-    // hydrostatic reconstruction in FP64 (eta = z + eta0)
-    const double K = P.eta0 + (double)fminf(a.H, b.H);
-    const double h0d = fmax((double)a.z + K, 0.0), h1d = fmax((double)b.z + K, 0.0);
-    const float h0 = (float)h0d, h1 = (float)h1d;
-    const float deta = (float)(h1d - h0d);
+    // hydrostatic reconstruction h* = max(eta + min(H_a, H_b), 0), eta = z + eta0:
+    // on an edge that is wet by a clear margin on both sides the depths are
+    // formed in FP32 and their difference is the exact difference of the
+    // surface deviations; otherwise (fronts) both are evaluated in FP64.
+    const float Hm = fminf(a.H, b.H);
+    const float Kf = P.eta0f + Hm;
+    float h0, h1, deta;
+    if (a.z + Kf > kWetMarginf && b.z + Kf > kWetMarginf) {
+        h0 = a.z + Kf;
+        h1 = b.z + Kf;
+        deta = b.z - a.z;
+    } else {
+        const double K = P.eta0 + (double)Hm;
+        const double h0d = fmax((double)a.z + K, 0.0), h1d = fmax((double)b.z + K, 0.0);
+        h0 = (float)h0d;
+        h1 = (float)h1d;
+        deta = (float)(h1d - h0d);
+    }
     float F0[5], F1[5];
     F0[0] = h0 * u0;
     F0[1] = F0[0] * u0;

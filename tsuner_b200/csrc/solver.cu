@@ -136,6 +136,7 @@ static void fill_phys(TsuSolver *s) {
     P.grass_ag = sw->grass_ag;
     Phys32 &Q = s->phys32;
     Q.eta0 = sw->eta0;
+    Q.eta0f = (float)sw->eta0;
     Q.FR = (float)p->FR;
     Q.eps_h = (float)p->epsilon_h;
     Q.Opar = (float)p->Opar;

@@ -66,11 +66,28 @@ __device__ __forceinline__ void recon32(const Phys32 &P, const float *s, int c, 
     const float Hi = s[PS + c], Hl = s[PS + l], Hr = s[PS + r];
     float dh = limiter32(hi - hl, hr - hi);
     if (0.5f * fabsf(dh) > hi) dh = copysignf(2.f * hi, dh);
-    // hydrostatic eta slope in FP64 (GPU/Reconstructor.cu:157-162)
-    double K = P.eta0 + (double)fminf(Hl, Hi);
-    float dl = (float)(fmax((double)zi + K, 0.0) - fmax((double)zl + K, 0.0));
-    K = P.eta0 + (double)fminf(Hr, Hi);
-    float dr = (float)(fmax((double)zr + K, 0.0) - fmax((double)zi + K, 0.0));
+    // hydrostatic eta slope (GPU/Reconstructor.cu:157-162): differences of
+    // max(eta + min(H), 0); exact z differences when both terms are clearly
+    // wet, FP64 otherwise
+    float dl, dr;
+    {
+        const float Hm = fminf(Hl, Hi), Kf = P.eta0f + Hm;
+        if (zi + Kf > kWetMarginf && zl + Kf > kWetMarginf) {
+            dl = zi - zl;
+        } else {
+            const double K = P.eta0 + (double)Hm;
+            dl = (float)(fmax((double)zi + K, 0.0) - fmax((double)zl + K, 0.0));
+        }
+    }
+    {
+        const float Hm = fminf(Hr, Hi), Kf = P.eta0f + Hm;
+        if (zr + Kf > kWetMarginf && zi + Kf > kWetMarginf) {
+            dr = zr - zi;
+        } else {
+            const double K = P.eta0 + (double)Hm;
+            dr = (float)(fmax((double)zr + K, 0.0) - fmax((double)zi + K, 0.0));
+        }
+    }
     deta = limiter32(dl, dr);
     const float dz = dh - deta;
     fm.h = hi - 0.5f * dh;
@@ -154,6 +171,12 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
 #pragma unroll
         for (int f = 0; f < 5; f++) v0[f] = V0[f * plane + gown];
     }
+    float ex_h = 0.f, ex_b = 0.f, ex_e = 0.f;  // running extrema, loaded early
+    if (LAST && own) {
+        ex_h = A.hmax[gown];
+        ex_b = A.bmin[gown];
+        ex_e = A.eta_max[gown];
+    }
     __syncthreads();
     const int cidx = (ty + 2) * LX + (tx + 2);
     float vc[5];
@@ -166,7 +189,9 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
 
     // ---- phase 2: depth (FP64 island), velocity, concentration per cell
     for (int idx = tid; idx < PS; idx += NT) {
-        const float h = (float)depth64(sV[idx], sV[PS + idx], eta0);
+        const float zz = sV[idx], HH = sV[PS + idx];
+        const float hs = zz + (P.eta0f + HH);  // FP32 when clearly wet, FP64 near dryness
+        const float h = (hs > kWetMarginf) ? hs : (float)depth64(zz, HH, eta0);
         float ux, uy, m;
         velocity32(h, sV[2 * PS + idx], sV[3 * PS + idx], ux, uy, m);
         sV[5 * PS + idx] = h;
@@ -426,10 +451,10 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
         Vout[4 * plane + gown] = hc;
         if (LAST) {
             if (h > P.eps_h) {
-                A.hmax[gown] = fmaxf(A.hmax[gown], h);
-                A.eta_max[gown] = fmaxf(A.eta_max[gown], (float)((double)z + eta0));
+                A.hmax[gown] = fmaxf(ex_h, h);
+                A.eta_max[gown] = fmaxf(ex_e, (float)((double)z + eta0));
             }
-            A.bmin[gown] = fmaxf(A.bmin[gown], H);
+            A.bmin[gown] = fmaxf(ex_b, H);
             const float d = cfl_dt32(P, h, qx, qy);
             if (!isnan(d)) dtcell = d;
             mass = fmax(hd, 0.0);
@@ -470,20 +495,35 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
         if (sLast) {
             __threadfence();
             const unsigned nb = gridDim.x * gridDim.y;
-            double mm = CUDART_INF;
-            for (unsigned i = tid; i < nb; i += NT) mm = fmin(mm, __ldcg(A.partials + i));
+            // every thread owns a fixed strided subset and the tree below has a
+            // fixed shape, so the FP64 sums do not depend on CTA timing
+            double mm = CUDART_INF, ms = 0.0, sd = 0.0;
+            for (unsigned i = tid; i < nb; i += NT) {
+                mm = fmin(mm, __ldcg(A.partials + i));
+                ms += __ldcg(A.partials + nb + i);
+                sd += __ldcg(A.partials + 2 * nb + i);
+            }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) mm = fmin(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+            for (int o = 16; o > 0; o >>= 1) {
+                mm = fmin(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+                ms += __shfl_xor_sync(0xffffffffu, ms, o);
+                sd += __shfl_xor_sync(0xffffffffu, sd, o);
+            }
             __syncthreads();
-            if ((tid & 31) == 0) sRed[tid >> 5] = mm;
+            if ((tid & 31) == 0) {
+                sRed[tid >> 5] = mm;
+                sRed[kWarps + (tid >> 5)] = ms;
+                sRed[2 * kWarps + (tid >> 5)] = sd;
+            }
             __syncthreads();
             if (tid == 0) {
-                for (int w = 0; w < kWarps; w++) mm = fmin(mm, sRed[w]);
-                // sums in a fixed order: deterministic FP64 totals
-                double ms = 0.0, sd = 0.0;
-                for (unsigned i = 0; i < nb; i++) {
-                    ms += __ldcg(A.partials + nb + i);
-                    sd += __ldcg(A.partials + 2 * nb + i);
+                mm = sRed[0];
+                ms = sRed[kWarps];
+                sd = sRed[2 * kWarps];
+                for (int w = 1; w < kWarps; w++) {
+                    mm = fmin(mm, sRed[w]);
+                    ms += sRed[kWarps + w];
+                    sd += sRed[2 * kWarps + w];
                 }
                 A.scal[SC_T] = t + dtd;
                 A.scal[SC_DT] = finalize_dt(mm, (long long)npx * npy);
