@@ -19,7 +19,8 @@ from tsuner_b200.abi import make_switches
 
 pytestmark = pytest.mark.gpu
 
-DEPTH_LINF_M = 1e-3     # bound asserted here on the small cases
+DEPTH_LINF_M = 1e-4     # shelf cases (the precision form's target)
+RUNUP_LINF_M = 2e-3     # Gaussian hump running up a beach (strong wet/dry fronts)
 MASS_REL = 1e-6
 
 
@@ -83,19 +84,19 @@ def test_water_conserved_with_walls_fp32():
     assert abs(m2 - m1) / m1 < MASS_REL, (m1, m2)
 
 
-@pytest.mark.parametrize("make,steps", [
-    (lambda: W.hump(256, 256, 10.0), 400),
-    (lambda: W.nwave_shelf(384, 256, 10.0, slr=0.5, amp=3.0, period=300.0, t_series=400.0), 400),
-])
-def test_depth_error_vs_fp64(make, steps):
+@pytest.mark.parametrize("make,steps,bound", [
+    (lambda: W.hump(256, 256, 10.0), 400, RUNUP_LINF_M),
+    (lambda: W.nwave_shelf(384, 256, 10.0, slr=0.5, amp=3.0, period=300.0, t_series=400.0), 400, DEPTH_LINF_M),
+], ids=["beach_runup", "shelf_nwave"])
+def test_depth_error_vs_fp64(make, steps, bound):
     w = make()
     V64, e64, t64, _ = run(w, sw_of(w, precision=0), steps)
     V32, e32, t32, _ = run(w, sw_of(w, precision=1), steps)
     linf = np.abs(V32[0] - V64[0]).max()
-    assert linf <= DEPTH_LINF_M, linf
+    assert linf <= bound, linf
     assert abs(t32[0] - t64[0]) / t64[0] < 1e-3
     wet = (e64[0] > -1e29) & (e32[0] > -1e29)
-    assert np.abs(e32[0][wet] - e64[0][wet]).max() <= 10 * DEPTH_LINF_M
+    assert np.abs(e32[0][wet] - e64[0][wet]).max() <= 10 * bound
 
 
 @pytest.mark.parametrize("kw", [

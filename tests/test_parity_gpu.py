@@ -60,23 +60,23 @@ def rel_err(a, b):
     return np.abs(a - b).max() / scale
 
 
-def assert_parity(new, ref, eps_h, exact=True, extrema=True):
+def assert_parity(new, ref, eps_h, exact=True, extrema=True, tol=REL_TOL):
     assert np.array_equal(new["V"][0] > eps_h, ref["V"][0] > eps_h), "wet/dry flags differ"
     for f, name in enumerate(FIELDS):
         e = rel_err(new["V"][f], ref["V"][f])
-        assert e <= REL_TOL, "%s rel err %.3e" % (name, e)
+        assert e <= tol, "%s rel err %.3e" % (name, e)
         if exact:
             assert np.array_equal(new["V"][f], ref["V"][f]), "%s not value-identical (rel %.3e)" % (name, e)
     if extrema:
         for k in ("hmax", "bmin", "eta_max"):
-            assert rel_err(new[k], ref[k]) <= REL_TOL, k
+            assert rel_err(new[k], ref[k]) <= tol, k
             if exact:
                 assert np.array_equal(new[k], ref[k]), k
     if exact:
         assert new["t"] == ref["t"] and new["dt"] == ref["dt"]
     else:
-        assert abs(new["t"] - ref["t"]) <= REL_TOL * abs(ref["t"])
-        assert abs(new["dt"] - ref["dt"]) <= REL_TOL * abs(ref["dt"])
+        assert abs(new["t"] - ref["t"]) <= tol * abs(ref["t"])
+        assert abs(new["dt"] - ref["dt"]) <= tol * abs(ref["dt"])
 
 
 # ------------------------------------------------------------- vs the oracle
@@ -159,8 +159,10 @@ def test_steps_are_graph_chunk_independent():
 need_ref = pytest.mark.skipif(not oracle.ref_available("default"), reason="oracle/_ref not built")
 
 
-def ref_vs_new(w, nsteps, variant, sw):
-    """Product vs the reference recipe build and vs its -nolto twin."""
+def ref_vs_new(w, nsteps, variant, sw, recipe_tol=REL_TOL):
+    """Product vs the reference recipe build and vs its -nolto twin.  The
+    product must equal the -nolto build value for value; the recipe build
+    within `recipe_tol` relative per field (its LTO rounding differs)."""
     if not (oracle.ref_available(variant) and oracle.ref_available(variant + "-nolto")):
         pytest.skip("reference variant %s not built" % variant)
     CC, tCC = (w.CC, w.tCC) if sw.read_files else (None, None)
@@ -171,7 +173,7 @@ def ref_vs_new(w, nsteps, variant, sw):
     pin = oracle.ref_run(variant + "-nolto", w.p, w.V, w.mask, CC, tCC, nsteps)
     assert ref["steps"] == pin["steps"] == nsteps
     assert_parity(new, pin, w.p.epsilon_h, exact=True)
-    assert_parity(new, ref, w.p.epsilon_h, exact=False)
+    assert_parity(new, ref, w.p.epsilon_h, exact=False, tol=recipe_tol)
     return new, ref
 
 
@@ -195,9 +197,12 @@ def test_nwave_vs_reference_build():
 
 @need_ref
 def test_config2_slice_4096_vs_reference_build():
-    """Full-size 4096^2 shelf with the N-wave series and harbour mask, 40 steps."""
+    """Full-size 4096^2 shelf with the N-wave series and harbour mask, 40 steps.
+    Value-identical to the -nolto reference build; the recipe (-dlto) build of
+    the same sources drifts from both by up to 6.4e-12 relative in qx here
+    (its link-time code generation rounds differently), so it is held to 1e-10."""
     w = W.nwave_shelf(4096, 4096, 5.0)
-    ref_vs_new(w, 40, "default", w.sw)
+    ref_vs_new(w, 40, "default", w.sw, recipe_tol=1e-10)
 
 
 @pytest.mark.parametrize("variant,sw", [
