@@ -191,6 +191,27 @@ int tsu_last_step_launches(TsuSolver *s, long *launches);
 /* Device pointer of the current state (plane-major, row pitch in elements). */
 int tsu_state_device(TsuSolver *s, void **ptr, long *pitch_elems, long *plane_elems,
                      int *elem_bytes);
+/* CFL time step of an FP64 state that the caller already holds in device
+ * memory, computed without any device allocation by the library.  No
+ * counterpart in the reference (its MinReduction works on a buffer that
+ * TSUNER() allocates).  It is for callers that cannot let a library call
+ * cudaMalloc: a host framework that owns every device byte through its own
+ * pool, code being captured into a CUDA graph (allocation is not allowed
+ * there), or a long-running service that forbids allocation after start-up.
+ * d_h, d_qx, d_qy: device planes of p->npy rows, row pitch `pitch_elems`
+ * doubles; d_dt: one device double that receives the step, with the same
+ * value tsu_reset() computes (GetDeltaT + MinReduction of the reference,
+ * float-rounded above 4096 cells).  `stream` is a cudaStream_t (NULL = the
+ * default stream); the call only enqueues work.
+ * The per-CTA partial minima live in a fixed file-scope device array of
+ * 16384 entries (~128 KiB, held by every GPU that loads the library until
+ * exit), so grids above 16384 CTAs of 32 x 8 cells (4,194,304 cells) are
+ * rejected with TSU_ERR_INVALID and a message.  The first call on a device
+ * looks up the array's device address on that device (make that first call
+ * before any stream capture).  Every call shares the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+int tsu_cfl_dt_noalloc(const double *d_h, const double *d_qx, const double *d_qy, long pitch_elems,
+                       const SimParams *p, double *d_dt, void *stream);
 const char *tsu_strerror(int code);
 /* Detail text of the last failing call on this thread ("" if none). */
 const char *tsu_last_error(void);

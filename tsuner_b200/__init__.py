@@ -29,7 +29,7 @@ EXPORTS = [
     "tsu_create", "tsu_destroy", "tsu_set_state", "tsu_set_mask", "tsu_set_boundary_series",
     "tsu_reset", "tsu_step", "tsu_run_until", "tsu_sync", "tsu_get_state", "tsu_get_extrema",
     "tsu_get_time", "tsu_get_sums", "tsu_get_consts", "tsu_last_step_ms", "tsu_last_step_launches",
-    "tsu_state_device", "tsu_strerror", "tsu_last_error", "tsu_version", "tsu_struct_sizes",
+    "tsu_state_device", "tsu_cfl_dt_noalloc", "tsu_strerror", "tsu_last_error", "tsu_version", "tsu_struct_sizes",
 ]
 
 
@@ -74,6 +74,7 @@ def lib():
             "tsu_last_step_launches": ([vp, C.POINTER(C.c_long)], C.c_int),
             "tsu_state_device": ([vp, C.POINTER(vp), C.POINTER(C.c_long), C.POINTER(C.c_long),
                                   C.POINTER(C.c_int)], C.c_int),
+            "tsu_cfl_dt_noalloc": ([vp, vp, vp, C.c_long, C.POINTER(SimParams), vp, vp], C.c_int),
             "tsu_strerror": ([C.c_int], C.c_char_p),
             "tsu_last_error": ([], C.c_char_p),
             "tsu_version": ([], C.c_char_p),

@@ -26,6 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 UNIT_FLAGS = {
     "stage64.cu": ["-fmad=false"],
     "solver.cu": ["-fmad=false"],
+    "noalloc.cu": ["-fmad=false"],
     # FP32 precision form: single precision may contract and use the hardware
     # approximations; its FP64 islands are unaffected by this flag.
     "stage32.cu": ["-use_fast_math"],
