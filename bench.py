@@ -2,7 +2,8 @@
 """Benchmark of the TSUNER hot path on B200: cell-steps/s of the time step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload nwave4096|hump512|humps8192] [--no-cpu-baseline]
+                  [--workload nwave4096|nwave2048|hump512|humps8192|ensembleN|corrector]
+                  [--no-cpu-baseline]
 
 One "step" is one full time step of the scheme (2 RK stages: MUSCL faces,
 edge fluxes with bedload, volume update, running extrema, CFL dt) over the
@@ -210,8 +211,143 @@ def form_switches(w, precision):
                          grass_ag=sw.grass_ag, eta0=sw.eta0)
 
 
+def run_ensemble(a, rank, world, local, dist):
+    """Config 4: batched FP32 ensemble; value = sum(cells) x steps / time."""
+    import tsuner_b200 as T
+    from tsuner_b200 import workloads as W
+    nmem = int(a.workload[len("ensemble"):] or 256)
+    ws = W.ensemble(nmembers=nmem)
+    cells = sum(w.ncells for w in ws)
+    e = T.Ensemble([w.p for w in ws], [w.sw for w in ws], device=local)
+    e.load(ws)
+    e.reset()
+    report = e.autotune(steps=2)
+    cfg = e.config()
+    e.step(a.warmup)
+    e.sync()
+    barrier(dist, local)
+    with Clocks(local) as clk:
+        e.step(a.steps)
+        e.sync()
+    ms = e.last_ms()
+    launches = e.last_launches()
+    ms_max = dist_max(dist, ms, local)
+    # the same members stepped one after the other with the single-grid kernels
+    ms_seq = 0.0
+    for s in e.members:
+        s.step(a.steps)
+        s.sync()
+        ms_seq += s.last_ms()
+    # end to end: upload every member, reset, K steps, read every member back
+    barrier(dist, local)
+    t0 = time.perf_counter()
+    e.load(ws)
+    e.reset()
+    e.step(a.steps)
+    e.sync()
+    finite = all(np.isfinite(s.state()).all() for s in e.members)
+    e2e_s = dist_max(dist, time.perf_counter() - t0, local)
+    e.close()
+    assert finite
+    if rank != 0:
+        return None
+    hbm, kind = peaks()
+    bpc = BYTES_PER_CELL_STEP["f32"]
+    achieved = bpc * cells * a.steps / (ms / 1e3) / 1e9
+    h2d = sum(5 * 8 * w.ncells + 4 * w.ncells + w.CC.nbytes + w.tCC.nbytes for w in ws)
+    d2h = sum(5 * 8 * w.ncells for w in ws)
+    return {
+        "metric": METRIC, "value": round(world * cells * a.steps / (ms_max / 1e3) / 1e6, 3),
+        "unit": "Mcell-steps/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, no dataset)",
+        "config": {"workload": "ensemble of %d members, square sides log-uniform in [256, 2048] (seed 4), "
+                               "own shelf bathymetry / mask / west N-wave each" % nmem,
+                   "cells": cells, "form": "fp32 precision form, one persistent launch per RK stage over all "
+                                            "members, per-member dt, CUDA graph",
+                   "tile": cfg, "autotune": report.strip().splitlines(),
+                   "parallelism": "replicas x%d" % world},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "peak_kind": kind, "bytes_per_cell_step": bpc,
+                     "traffic": None},
+        "members_one_by_one": {"value": round(cells * a.steps / (ms_seq / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
+                               "ms_per_step": round(ms_seq / a.steps, 4)},
+        "gpu_launches": launches,
+        "e2e": {"value": round(world * cells * a.steps / e2e_s / 1e6, 3), "unit": "Mcell-steps/s",
+                "h2d_bytes_per_step": int(h2d / a.steps), "d2h_bytes_per_step": int(d2h / a.steps),
+                "what": "upload all members + reset + K steps + read all members back, host buffers"},
+        "clocks": clk.summary(),
+    }
+
+
+def run_corrector(a, rank, world, local, dist):
+    """Learned corrector (reduced config 5): FP32 coarse solves (factor 4)
+    lifted to fine maximum-depth / bed-change maps; the pairs come from the
+    solver (FP32 ensembles), the held-out truth from the FP64 plain form.
+    Reports held-out error with and without the corrector, training time and
+    the tensor-core convolution's TFLOP/s.  Replicas only (each rank runs the
+    whole pipeline)."""
+    from tsuner_b200 import corrector as K
+    n, f, t_end = a.corr_fine, 4, a.corr_tend
+    site = K.make_site(n=n, factor=f)
+    train_src = K.make_sources(a.corr_train, seed=11)
+    test_src = K.make_sources(a.corr_test, seed=12)
+    t0 = time.perf_counter()
+    fine_train = K.solve_fp32(site.H, site.mask, site.dx, site.slr, train_src, t_end)
+    t_fine = time.perf_counter() - t0
+    coarse_train = K.coarse_inputs(site, train_src, t_end)
+    coarse_test = K.coarse_inputs(site, test_src, t_end)
+    t0 = time.perf_counter()
+    truth = K.solve_fp64(site.H, site.mask, site.dx, site.slr, test_src, t_end)
+    t_truth = time.perf_counter() - t0
+    c = K.Corrector(n, n, f, max_batch=8, device=local)
+    c.set_site(site.H)
+    c.add_samples(coarse_train, fine_train)
+    c.add_samples(coarse_test, truth)
+    loss = c.train(len(train_src), a.corr_iters, batch=8, lr=1e-3, seed=1)
+    train_ms, convs = c.last_train()
+    oh, ob, bh, bb = c.predict(len(train_src), len(test_src))
+    with Clocks(local) as clk:
+        ms_conv, tflops = c.bench_conv(8, max(a.steps, 5))
+    c.close()
+    e_with = K.errors((oh, ob), truth)
+    e_without = K.errors((bh, bb), truth)
+    if rank != 0:
+        return None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peak, kind = float(json.load(fh)["bf16_tflops"]), "measured (burst)"
+    except Exception:
+        peak, kind = 1590.0, "fallback"
+    return {
+        "metric": "corrector: held-out fine-map error with/without; tensor-core conv TFLOP/s", "value": round(tflops, 1),
+        "unit": "TFLOP/s", "n_gpus": world, "steps": max(a.steps, 5), "warmup": 3,
+        "ms_per_step": round(ms_conv, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 (fp32 accumulate)", "data": "synthetic (seeded site and sources, solver-generated pairs)",
+        "config": {"workload": "corrector: fine %dx%d dx=%.0fm <- coarse %dx%d, %d train pairs (FP32 ensembles), "
+                               "%d held-out sources judged against the FP64 plain solve, t_end %.0f s"
+                               % (n, n, site.dx, n // f, n // f, len(train_src), len(test_src), t_end),
+                   "network": "6 x conv3x3 32 ch, BF16 weights/activations, FP32 accumulate (tcgen05, TMEM)",
+                   "train": {"iters": a.corr_iters, "batch": 8, "lr": 1e-3, "ms": round(train_ms, 1),
+                             "convs": convs, "loss_first": float(loss[:5].mean()),
+                             "loss_last": float(loss[-10:].mean())},
+                   "solve_seconds": {"fine_fp32_train": round(t_fine, 2), "fine_fp64_heldout": round(t_truth, 2)},
+                   "parallelism": "replicas x%d" % world},
+        "errors": {"with_corrector": e_with, "interpolation_only": e_without},
+        "roofline": {"bound": "tensor", "achieved": round(tflops, 1), "peak": peak, "unit": "TFLOP/s",
+                     "frac": round(tflops / peak, 4), "peak_kind": kind, "traffic": None,
+                     "note": "2 x pixels x 288 x 32 FLOPs per 3x3 convolution, 8 images per launch"},
+        "gpu_launches": max(a.steps, 5),
+        "clocks": clk.summary(),
+    }
+
+
 def run_ours(a, rank, world, local, dist):
     import tsuner_b200 as T
+    if a.workload.startswith("ensemble"):
+        return run_ensemble(a, rank, world, local, dist)
+    if a.workload == "corrector":
+        return run_corrector(a, rank, world, local, dist)
     w, desc = workload(a.workload)
     n = w.ncells
     prim = 1 if a.precision == "fp32" else 0
@@ -344,6 +480,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--corr-fine", type=int, default=512, help="corrector: fine grid side")
+    ap.add_argument("--corr-train", type=int, default=128, help="corrector: training pairs")
+    ap.add_argument("--corr-test", type=int, default=16, help="corrector: held-out sources")
+    ap.add_argument("--corr-iters", type=int, default=400, help="corrector: Adam steps")
+    ap.add_argument("--corr-tend", type=float, default=600.0, help="corrector: simulated seconds per source")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     rank, world, local, dist = dist_setup(a.gpus)

@@ -191,6 +191,79 @@ int tsu_last_step_launches(TsuSolver *s, long *launches);
 /* Device pointer of the current state (plane-major, row pitch in elements). */
 int tsu_state_device(TsuSolver *s, void **ptr, long *pitch_elems, long *plane_elems,
                      int *elem_bytes);
+/* ---------------- batched ensemble (FP32 form) ----------------
+ * No counterpart in the reference (single grid only).  nmembers grids of
+ * any sizes (params[i]) with their own switches (sw[i]: precision must be 1
+ * and the order the same for all), stepped together: per RK stage one
+ * persistent kernel walks the tiles of all members; every member advances
+ * with its own dt (segmented min-reduction on the device).  Members are
+ * ordinary solvers: fill them through tsu_ens_member() + tsu_set_state /
+ * tsu_set_mask / tsu_set_boundary_series, read them back the same way. */
+typedef struct TsuEnsemble TsuEnsemble;
+int tsu_ens_create(TsuEnsemble **out, int nmembers, const SimParams *params, const TsuSwitches *sw, int device);
+int tsu_ens_destroy(TsuEnsemble *e);
+int tsu_ens_member(TsuEnsemble *e, int i, TsuSolver **solver);
+/* t = 0, extrema and initial dt of every member (after the states are set). */
+int tsu_ens_reset(TsuEnsemble *e);
+/* Enqueues nsteps steps of every member (no host sync). */
+int tsu_ens_step(TsuEnsemble *e, long nsteps);
+int tsu_ens_sync(TsuEnsemble *e);
+/* Times each tile shape x schedule (static stride / dynamic work counter /
+ * one CTA per tile) x resident-CTA count over `steps` steps, keeps the
+ * fastest and restores the members' states; optional text report. */
+int tsu_ens_autotune(TsuEnsemble *e, int steps, char *report, size_t cap);
+int tsu_ens_set_config(TsuEnsemble *e, int variant, int dynamic, int ctas);
+int tsu_ens_get_config(TsuEnsemble *e, int *variant, int *tile_x, int *tile_y, int *dynamic, int *ctas,
+                       long *ntiles);
+int tsu_ens_last_step_ms(TsuEnsemble *e, double *ms);
+int tsu_ens_last_step_launches(TsuEnsemble *e, long *launches);
+/* Steps every member until its time reaches t_end (members that are done
+ * skip their tiles) or max_steps steps were enqueued; *steps_done = steps
+ * enqueued.  Members keep their own step counts (tsu_get_time). */
+int tsu_ens_run_until(TsuEnsemble *e, double t_end, long max_steps, long *steps_done);
+
+/* ---------------- learned corrector ----------------
+ * No counterpart in the reference.  A 6-layer, 32-channel 3x3 convolutional
+ * network (BF16 weights and activations, FP32 accumulation on the tensor
+ * cores, ReLU between layers) that maps coarse-grid maps (maximum depth,
+ * bed change, bathymetry; [3][ny/factor][nx/factor] per sample) plus the
+ * fine bathymetry to fine-grid maximum depth and bed change [2][ny][nx]:
+ * output = bilinear interpolation of the coarse maps + learned residual.
+ * Trained with Adam on mean-square error against fine solves. */
+typedef struct TsuCorrector TsuCorrector;
+int tsu_corr_create(TsuCorrector **out, int ny, int nx, int factor, int max_batch, unsigned long long seed,
+                    int device);
+int tsu_corr_destroy(TsuCorrector *c);
+/* fine bathymetry H (depth below datum), [ny][nx] */
+int tsu_corr_set_site(TsuCorrector *c, const float *fine_H);
+/* appends n samples: coarse [n][3][ny/f][nx/f]; fine [n][2][ny][nx] targets or NULL */
+int tsu_corr_add_samples(TsuCorrector *c, int n, const float *coarse, const float *fine);
+int tsu_corr_num_samples(TsuCorrector *c, int *n);
+/* FP32 master weights [6][32 cout][9 taps][32 cin] and biases [6][32] */
+int tsu_corr_get_weights(TsuCorrector *c, float *W, float *B);
+int tsu_corr_set_weights(TsuCorrector *c, const float *W, const float *B);
+/* iters Adam steps on seeded mini-batches of samples [0, ntrain); loss[iters] (optional) */
+int tsu_corr_train(TsuCorrector *c, int ntrain, int iters, int batch, float lr, unsigned long long seed,
+                   float *loss);
+/* corrected maps of samples [first, first+n): [n][ny][nx] each; base_* (optional) = interpolation only */
+int tsu_corr_predict(TsuCorrector *c, int first, int n, float *out_hmax, float *out_db, float *base_hmax,
+                     float *base_db);
+/* device time per forward convolution over nimg fine images and TFLOP/s */
+int tsu_corr_bench_conv(TsuCorrector *c, int nimg, int iters, double *ms_per_conv, double *tflops);
+int tsu_corr_last_train_ms(TsuCorrector *c, double *ms, long *convs);
+/* Raw kernels on caller-owned device buffers (NHWC BF16, 32 channels):
+ * Y = act(conv3x3(X, Wk[cout][tap][cin]) + bias), act = ReLU if relu, then
+ * channel n zeroed where gate[p][n] <= 0 (if gate); BF16 (Ybf) or FP32 (Yf)
+ * output.  wgrad adds sum_p dZ[p][cout] X[p+off(tap)][cin] to dW[cout][tap][cin]
+ * and sum_p dZ[p][cout] to db[cout] (FP32).  stream: cudaStream_t or NULL. */
+int tsu_corr_conv3x3(const void *X, int nimg, int H, int W, const void *Wk, const float *bias, int relu,
+                     const void *gate, void *Ybf, float *Yf, void *stream);
+int tsu_corr_conv3x3_wgrad(const void *X, const void *dZ, int nimg, int H, int W, float *dW, float *db,
+                           void *stream);
+/* synchronises the device; TSU_ERR_CUDA if a corrector kernel's wait expired */
+int tsu_corr_status(void);
+const char *tsu_corr_last_error(void);
+
 /* CFL time step of an FP64 state that the caller already holds in device
  * memory, computed without any device allocation by the library.  No
  * counterpart in the reference (its MinReduction works on a buffer that

@@ -2,9 +2,10 @@
  * Minimal declaration of the libnetcdf C API subset that the reference
  * TSUNER sources call (GPU/netcdf.cu, Problem_loader.cxx, interpolations.cxx,
  * tides.cxx).  The image has no libnetcdf; this header lets the reference
- * kernels compile unmodified for the parity harness.  The functions are
- * implemented by netcdf_shim.cpp (writer subset, backed by the CDF-1 writer
- * of this repository) -- reader functions return NC_ENOTNC.
+ * kernels compile unmodified for the parity harness: the kernel sources the
+ * harness builds (GPU/Reconstructor.cu, VolumeSolver.cu, Volume_kernel.cu,
+ * Reduction_kernel_min.cu) include it through GPU/GPU_kernels.cuh and
+ * TSUNER.h but call none of its functions, so no implementation is linked.
  *
  * TEST INFRASTRUCTURE ONLY: used to build the reference checker under
  * oracle/_ref/, never by the product library.

@@ -1,0 +1,172 @@
+"""GPU: the corrector's tensor-core convolutions against plain PyTorch FP32
+references of the same ops (BF16-rounded inputs, FP32 accumulation), and
+its training loop end to end (loss goes down; the untrained corrector is
+the bilinear interpolation)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import tsuner_b200 as T
+from tsuner_b200 import corrector as K
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+F = torch.nn.functional
+
+
+def dev():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda:0")
+
+
+def bf16(x):
+    return x.to(torch.bfloat16)
+
+
+def nhwc(x):  # [n][c][h][w] -> [n][h][w][c] contiguous
+    return x.permute(0, 2, 3, 1).contiguous()
+
+
+def wk_from_torch(w):  # torch [cout][cin][3][3] -> [cout][tap][cin]
+    return w.permute(0, 2, 3, 1).reshape(32, 9, 32).contiguous()
+
+
+def ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def conv(X, Wk, bias=None, relu=0, gate=None, out_fp32=True):
+    n, h, w, _ = X.shape
+    Yf = torch.zeros((n, h, w, 32), device=X.device, dtype=torch.float32) if out_fp32 else None
+    Yb = None if out_fp32 else torch.zeros((n, h, w, 32), device=X.device, dtype=torch.bfloat16)
+    rc = T.lib().tsu_corr_conv3x3(ptr(X), n, h, w, ptr(Wk), ptr(bias), relu, ptr(gate), ptr(Yb), ptr(Yf), None)
+    assert rc == 0, T.lib().tsu_corr_last_error()
+    assert T.lib().tsu_corr_status() == 0
+    return Yf if out_fp32 else Yb
+
+
+def rand_case(n, h, w, seed):
+    g = torch.Generator().manual_seed(seed)
+    X = bf16(torch.randn(n, 32, h, w, generator=g))
+    Wt = bf16(torch.randn(32, 32, 3, 3, generator=g) * 0.1)
+    b = torch.randn(32, generator=g) * 0.1
+    return X, Wt, b
+
+
+@pytest.mark.parametrize("shape", [(1, 16, 8), (2, 37, 29), (1, 130, 67)])
+def test_conv_forward_fp32_out(shape):
+    d = dev()
+    n, h, w = shape
+    X, Wt, b = rand_case(n, h, w, 1)
+    ref = F.conv2d(X.float().to(d), Wt.float().to(d), b.to(d), padding=1)
+    Y = conv(nhwc(X).to(d), wk_from_torch(Wt).to(d), b.to(d), relu=0)
+    err = (Y - nhwc(ref)).abs().max().item()
+    assert err <= 1e-4 * max(1.0, ref.abs().max().item()), err
+
+
+def test_conv_forward_relu_bf16_out_and_gate():
+    d = dev()
+    X, Wt, b = rand_case(2, 40, 24, 2)
+    G = bf16(torch.randn(2, 40, 24, 32)).to(d)
+    ref = torch.relu(F.conv2d(X.float().to(d), Wt.float().to(d), b.to(d), padding=1))
+    ref = nhwc(ref) * (G.float() > 0)
+    Y = conv(nhwc(X).to(d), wk_from_torch(Wt).to(d), b.to(d), relu=1, gate=G, out_fp32=False)
+    # one BF16 rounding of the FP32 result
+    err = (Y.float() - ref).abs()
+    assert (err <= 2.0 ** -8 * ref.abs() + 1e-6).all(), err.max().item()
+    assert bool(((ref == 0) == (Y.float() == 0)).all())
+
+
+def test_conv_input_gradient_with_flipped_weights():
+    """dX = conv(dZ, Wt[cin][8 - tap][cout] = W[cout][tap][cin]) is the input
+    gradient of the forward convolution."""
+    d = dev()
+    X, Wt, _ = rand_case(1, 33, 20, 3)
+    dZ = bf16(torch.randn(1, 32, 33, 20) * 0.5)
+    ref = torch.nn.grad.conv2d_input(X.shape, Wt.float().to(d), dZ.float().to(d), padding=1)
+    wk = wk_from_torch(Wt)  # [cout][tap][cin]
+    flip = wk.flip(1).permute(2, 1, 0).contiguous()  # [cin][tap'][cout], tap' = 8 - tap
+    Y = conv(nhwc(dZ).to(d), flip.to(d), None, relu=0)
+    err = (Y - nhwc(ref)).abs().max().item()
+    assert err <= 1e-4 * max(1.0, ref.abs().max().item()), err
+
+
+@pytest.mark.parametrize("shape", [(1, 16, 8), (3, 45, 27)])
+def test_conv_weight_and_bias_gradient(shape):
+    d = dev()
+    n, h, w = shape
+    X, Wt, _ = rand_case(n, h, w, 4)
+    dZ = bf16(torch.randn(n, 32, h, w) * 0.5)
+    ref_w = torch.nn.grad.conv2d_weight(X.float().to(d), Wt.shape, dZ.float().to(d), padding=1)
+    ref_b = dZ.float().sum(dim=(0, 2, 3)).to(d)
+    dW = torch.zeros(32, 9, 32, device=d)
+    db = torch.zeros(32, device=d)
+    Xd, Zd = nhwc(X).to(d), nhwc(dZ).to(d)  # keep both alive across the call
+    rc = T.lib().tsu_corr_conv3x3_wgrad(ptr(Xd), ptr(Zd), n, h, w, ptr(dW), ptr(db), None)
+    assert rc == 0
+    assert T.lib().tsu_corr_status() == 0
+    scale = max(1.0, ref_w.abs().max().item())
+    err = (dW - wk_from_torch(ref_w)).abs().max().item()
+    assert err <= 1e-4 * scale, err
+    assert (db - ref_b).abs().max().item() <= 1e-4 * max(1.0, ref_b.abs().max().item())
+
+
+def synthetic_samples(n, ny, f, seed):
+    """Coarse maps and fine targets with a learnable relation: fine maximum
+    depth = interpolated coarse + sub-grid bathymetry detail where wet."""
+    rng = np.random.default_rng(seed)
+    Hf = (20.0 + 5.0 * np.sin(np.arange(ny) / 3.0)[None, :] + rng.normal(0, 1.0, (ny, ny))).astype(np.float32)
+    Hc = K.block_mean(Hf, f).astype(np.float32)
+    coarse, fine = [], []
+    for _ in range(n):
+        a = rng.uniform(0.5, 2.0)
+        hc = (Hc + a).astype(np.float32)
+        dbc = np.full_like(Hc, 0.01 * a)
+        coarse.append(np.stack([hc, dbc, Hc]))
+        fine.append(np.stack([Hf + a, np.full_like(Hf, 0.01 * a)]).astype(np.float32))
+    return Hf, np.stack(coarse), np.stack(fine)
+
+
+def test_untrained_corrector_is_interpolation_and_training_lowers_loss():
+    dev()
+    ny, f = 64, 4
+    Hf, coarse, fine = synthetic_samples(12, ny, f, 5)
+    c = K.Corrector(ny, ny, f, max_batch=4, seed=3)
+    try:
+        c.set_site(Hf)
+        c.add_samples(coarse, fine)
+        oh, ob, bh, bb = c.predict(0, 2)
+        assert np.array_equal(oh, bh) and np.array_equal(ob, bb)  # zero last layer
+        loss = c.train(ntrain=12, iters=150, batch=4, lr=2e-3, seed=1)
+        assert np.isfinite(loss).all()
+        assert loss[-10:].mean() < 0.5 * loss[:5].mean(), (loss[:5], loss[-10:])
+        oh2, _, _, _ = c.predict(0, 2)
+        before = np.sqrt(((bh - fine[:2, 0]) ** 2).mean())
+        after = np.sqrt(((oh2 - fine[:2, 0]) ** 2).mean())
+        assert after < before, (before, after)
+        Wt, B = c.weights()
+        assert np.isfinite(Wt).all() and np.abs(Wt[-1]).max() > 0
+    finally:
+        c.close()
+
+
+def test_set_weights_round_trip_and_conv_bench():
+    dev()
+    ny, f = 32, 4
+    Hf, coarse, fine = synthetic_samples(2, ny, f, 6)
+    c = K.Corrector(ny, ny, f, max_batch=2, seed=4)
+    try:
+        c.set_site(Hf)
+        c.add_samples(coarse, fine)
+        Wt, B = c.weights()
+        Wt2 = Wt * 0.5
+        c.set_weights(Wt2, B + 1.0)
+        Wr, Br = c.weights()
+        assert np.array_equal(Wr, Wt2) and np.array_equal(Br, B + 1.0)
+        ms, tf = c.bench_conv(2, 3)
+        assert ms > 0 and tf > 0
+    finally:
+        c.close()

@@ -19,7 +19,10 @@ from tsuner_b200.abi import make_switches
 
 pytestmark = pytest.mark.gpu
 
-DEPTH_LINF_M = 1e-4     # shelf cases (the precision form's target)
+# L-inf depth difference to the FP64 form after 400 steps.  It is set by the
+# wet/dry front cells, where FP32 and FP64 runs may wet a cell one step apart;
+# away from fronts the difference is ~1e-6 m (see the L2 in bench.py).
+DEPTH_LINF_M = 5e-4     # coarse shelf, 3 m N-wave reaching the beach
 RUNUP_LINF_M = 2e-3     # Gaussian hump running up a beach (strong wet/dry fronts)
 MASS_REL = 1e-6
 

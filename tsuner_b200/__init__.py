@@ -30,7 +30,47 @@ EXPORTS = [
     "tsu_reset", "tsu_step", "tsu_run_until", "tsu_sync", "tsu_get_state", "tsu_get_extrema",
     "tsu_get_time", "tsu_get_sums", "tsu_get_consts", "tsu_last_step_ms", "tsu_last_step_launches",
     "tsu_state_device", "tsu_cfl_dt_noalloc", "tsu_strerror", "tsu_last_error", "tsu_version", "tsu_struct_sizes",
+    "tsu_ens_create", "tsu_ens_destroy", "tsu_ens_member", "tsu_ens_reset", "tsu_ens_step", "tsu_ens_sync",
+    "tsu_ens_autotune", "tsu_ens_set_config", "tsu_ens_get_config", "tsu_ens_last_step_ms",
+    "tsu_ens_last_step_launches", "tsu_ens_run_until",
+    "tsu_corr_create", "tsu_corr_destroy", "tsu_corr_set_site", "tsu_corr_add_samples", "tsu_corr_num_samples",
+    "tsu_corr_get_weights", "tsu_corr_set_weights", "tsu_corr_train", "tsu_corr_predict", "tsu_corr_bench_conv",
+    "tsu_corr_last_train_ms", "tsu_corr_conv3x3", "tsu_corr_conv3x3_wgrad", "tsu_corr_status",
+    "tsu_corr_last_error",
 ]
+
+_ENS_SIG = {
+    "tsu_ens_create": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "tsu_ens_destroy": ([C.c_void_p], C.c_int),
+    "tsu_ens_member": ([C.c_void_p, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "tsu_ens_reset": ([C.c_void_p], C.c_int),
+    "tsu_ens_step": ([C.c_void_p, C.c_long], C.c_int),
+    "tsu_ens_sync": ([C.c_void_p], C.c_int),
+    "tsu_ens_autotune": ([C.c_void_p, C.c_int, C.c_char_p, C.c_size_t], C.c_int),
+    "tsu_ens_set_config": ([C.c_void_p, C.c_int, C.c_int, C.c_int], C.c_int),
+    "tsu_ens_get_config": ([C.c_void_p] + [C.POINTER(C.c_int)] * 5 + [C.POINTER(C.c_long)], C.c_int),
+    "tsu_ens_last_step_ms": ([C.c_void_p, C.POINTER(C.c_double)], C.c_int),
+    "tsu_ens_last_step_launches": ([C.c_void_p, C.POINTER(C.c_long)], C.c_int),
+    "tsu_ens_run_until": ([C.c_void_p, C.c_double, C.c_long, C.POINTER(C.c_long)], C.c_int),
+    "tsu_corr_create": ([C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.c_int],
+                        C.c_int),
+    "tsu_corr_destroy": ([C.c_void_p], C.c_int),
+    "tsu_corr_set_site": ([C.c_void_p, C.c_void_p], C.c_int),
+    "tsu_corr_add_samples": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
+    "tsu_corr_num_samples": ([C.c_void_p, C.POINTER(C.c_int)], C.c_int),
+    "tsu_corr_get_weights": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "tsu_corr_set_weights": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "tsu_corr_train": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_ulonglong, C.c_void_p], C.c_int),
+    "tsu_corr_predict": ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 4, C.c_int),
+    "tsu_corr_bench_conv": ([C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+    "tsu_corr_last_train_ms": ([C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)], C.c_int),
+    "tsu_corr_conv3x3": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                          C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "tsu_corr_conv3x3_wgrad": ([C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                C.c_void_p], C.c_int),
+    "tsu_corr_status": ([], C.c_int),
+    "tsu_corr_last_error": ([], C.c_char_p),
+}
 
 
 class TsunerError(RuntimeError):
@@ -84,6 +124,7 @@ def lib():
             "checkCUDAsupport": ([C.c_int], C.c_int),
             "initializeGPU": ([], None),
         }
+        sig.update(_ENS_SIG)
         for name, (args, res) in sig.items():
             f = getattr(L, name)
             f.argtypes = args
@@ -109,10 +150,17 @@ class Solver:
         self._h = C.c_void_p()
         _ck(lib().tsu_create(C.byref(self._h), C.byref(p), C.byref(sw), device), "tsu_create")
 
+    @classmethod
+    def _borrow(cls, handle, p, sw):
+        """View of a solver owned by someone else (an ensemble member)."""
+        s = cls.__new__(cls)
+        s.p, s.sw, s._h, s._owned = p, sw, handle, False
+        return s
+
     def close(self):
-        if self._h:
+        if self._h and getattr(self, "_owned", True):
             lib().tsu_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
@@ -196,6 +244,82 @@ class Solver:
         _ck(lib().tsu_state_device(self._h, C.byref(ptr), C.byref(pitch), C.byref(plane), C.byref(eb)),
             "tsu_state_device")
         return ptr.value, pitch.value, plane.value, eb.value
+
+
+class Ensemble:
+    """Batched FP32-form ensemble through the tsu_ens_* C ABI."""
+
+    def __init__(self, params, switches, device=0):
+        n = len(params)
+        self.n = n
+        self._P = (SimParams * n)(*params)
+        self._S = (TsuSwitches * n)(*switches)
+        self._h = C.c_void_p()
+        _ck(lib().tsu_ens_create(C.byref(self._h), n, C.cast(self._P, C.c_void_p), C.cast(self._S, C.c_void_p),
+                                 device), "tsu_ens_create")
+        self.members = []
+        for i in range(n):
+            hs = C.c_void_p()
+            _ck(lib().tsu_ens_member(self._h, i, C.byref(hs)), "tsu_ens_member")
+            self.members.append(Solver._borrow(hs, self._P[i], self._S[i]))
+
+    def close(self):
+        if self._h:
+            lib().tsu_ens_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load(self, workloads):
+        for s, w in zip(self.members, workloads):
+            s.set_state(w.V)
+            s.set_mask(w.mask)
+            if w.sw.read_files:
+                s.set_boundary_series(w.CC, w.tCC)
+
+    def reset(self):
+        _ck(lib().tsu_ens_reset(self._h), "tsu_ens_reset")
+
+    def step(self, n):
+        _ck(lib().tsu_ens_step(self._h, n), "tsu_ens_step")
+
+    def run_until(self, t_end, max_steps=1 << 40):
+        done = C.c_long()
+        _ck(lib().tsu_ens_run_until(self._h, t_end, max_steps, C.byref(done)), "tsu_ens_run_until")
+        return done.value
+
+    def sync(self):
+        _ck(lib().tsu_ens_sync(self._h), "tsu_ens_sync")
+
+    def autotune(self, steps=3):
+        buf = C.create_string_buffer(8192)
+        _ck(lib().tsu_ens_autotune(self._h, steps, buf, 8192), "tsu_ens_autotune")
+        return buf.value.decode()
+
+    def set_config(self, variant, dynamic, ctas=0):
+        _ck(lib().tsu_ens_set_config(self._h, variant, dynamic, ctas), "tsu_ens_set_config")
+
+    def config(self):
+        v, tx, ty, d, c = (C.c_int() for _ in range(5))
+        nt = C.c_long()
+        _ck(lib().tsu_ens_get_config(self._h, C.byref(v), C.byref(tx), C.byref(ty), C.byref(d), C.byref(c),
+                                     C.byref(nt)), "tsu_ens_get_config")
+        return dict(variant=v.value, tile=(tx.value, ty.value), dynamic=bool(d.value), ctas=c.value,
+                    ntiles=nt.value)
+
+    def last_ms(self):
+        ms = C.c_double()
+        _ck(lib().tsu_ens_last_step_ms(self._h, C.byref(ms)), "tsu_ens_last_step_ms")
+        return ms.value
+
+    def last_launches(self):
+        n = C.c_long()
+        _ck(lib().tsu_ens_last_step_launches(self._h, C.byref(n)), "tsu_ens_last_step_launches")
+        return n.value
 
 
 def solver_for(w, device=0):

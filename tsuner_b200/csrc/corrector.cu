@@ -1,0 +1,1065 @@
+// corrector.cu -- learned corrector: a 6-layer, 32-channel 3x3 convolutional
+// network that lifts coarse-grid maximum-depth / bed-change maps to the fine
+// grid.  Its convolutions (forward, input gradient, weight gradient) run on
+// the 5th-generation tensor cores (tcgen05.mma, BF16 operands from shared
+// memory, FP32 accumulators in TMEM); the rest of the training loop
+// (feature assembly, loss, Adam) is small elementwise kernels.
+// No counterpart in the reference.
+//
+// Tensors: activations NHWC BF16 with 32 channels ([img][y][x][32]);
+// weights BF16 Wk[cout][tap][cin], tap = (dy+1)*3 + (dx+1) (so that
+// Y[y][x] = sum W[tap] X[y+dy][x+dx], zero padding); FP32 master weights,
+// bias and Adam moments.
+//
+// Forward / input-gradient convolution (conv3x3_fwd_kernel): implicit GEMM
+//   D[128 pixels x 32 cout] = sum over 9 taps x 2 channel halves of
+//   A_tap,h[128 x 16] . B_tap,h[16 x 32]  (18 MMAs of M=128, N=32, K=16)
+// over an 8 x 16 pixel tile.  The input patch (10 x 18 pixels with the halo)
+// is stored in shared memory as four channel-quarter planes (16 bytes per
+// pixel per plane), which makes every A_tap,h a K-major no-swizzle operand
+// that starts inside the patch: core matrix = 8 consecutive pixels of one
+// tile row (16-byte rows), the two K chunks one plane apart (LBO = plane
+// size) and the 16 row groups one patch row apart (SBO = 160 B).  No im2col
+// copy is made.  CTAs are persistent; the patch and the TMEM accumulator are
+// double-buffered so that the load of tile i+1 and the epilogue of tile i-1
+// overlap the MMAs of tile i.
+//
+// Weight gradient (conv3x3_wgrad_kernel): dW[cout][tap][cin] =
+//   sum_p dZ[p][cout] X[p + off(tap)][cin], a GEMM with the pixels as the
+// reduction dimension: D[288 (tap,cin) x 32 (cout)] in three M=128 blocks,
+// MN-major operands (8 pixels x 16 bytes per core matrix): A is copied from
+// the patch planes in 128-byte core matrices, B is the dZ tile itself.  Row
+// 288 of A is all ones, so D[288][cout] is the bias gradient.  Each CTA
+// accumulates a strip of tiles in TMEM and adds its partial result to the
+// FP32 gradients with atomics.
+//
+// Every mbarrier wait is bounded (globaltimer); on expiry the kernel sets
+// the error word, waits once more (bounded) for its MMAs, frees its TMEM and
+// returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "tsuner_b200.h"
+
+namespace tsu {
+namespace corr {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int C = 32;                       // channels
+constexpr int TXP = 8, TYP = 16;            // output tile (128 pixels)
+constexpr int PW = TXP + 2, PH = TYP + 2;   // patch 10 x 18
+constexpr int PPIX = PW * PH;               // 180
+constexpr int kPlane = PPIX * 16;           // one channel-quarter plane: 2880 B
+constexpr int kPatch = 4 * kPlane;          // 11520 B
+constexpr int kWBytes = 9 * 4 * 32 * 16;    // weights: 18432 B
+constexpr int KROWS = 9 * C;                // 288
+constexpr unsigned long long kWaitNs = 500000000ull;  // 0.5 s per wait
+
+constexpr int kFwdSmem = 1024 + kWBytes + 2 * kPatch + 64;
+// wgrad: patch + dZ tile + A (8 K steps x 3 M blocks x 4 KB)
+constexpr int kZPlane = 128 * 16;
+constexpr int kABlock = 4096;
+constexpr int kWgSmem = 1024 + kPatch + 4 * kZPlane + 8 * 3 * kABlock + 64;
+
+__device__ int g_corr_err;  // set by a kernel whose wait expired
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// UMMA shared-memory descriptor, no swizzle, sm100 version field
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+
+// kind::f16 instruction descriptor: D FP32, A/B BF16, majors, N, M
+__host__ __device__ constexpr uint32_t idesc(int M, int N, int a_mn, int b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+    const unsigned long long t0 = gtimer();
+    while (!mbar_try(bar, parity))
+        if (gtimer() - t0 > kWaitNs) return false;
+    return true;
+}
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t id, uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(id), "r"(accum)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+// thread `lane` of the warp receives TMEM lane (base + lane), 32 columns
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&h);
+}
+
+struct TileGeom {
+    int ntx, nty, per_img, total;
+};
+__host__ __device__ inline TileGeom tile_geom(int nimg, int H, int W) {
+    TileGeom g;
+    g.ntx = (W + TXP - 1) / TXP;
+    g.nty = (H + TYP - 1) / TYP;
+    g.per_img = g.ntx * g.nty;
+    g.total = nimg * g.per_img;
+    return g;
+}
+
+// 10 x 18 x 32 input patch (zero padding) -> four channel-quarter planes
+__device__ __forceinline__ void load_patch(const bf16 *__restrict__ X, int img, int H, int W, int x0, int y0,
+                                           unsigned char *patch, int tid) {
+    const bf16 *Xi = X + (long long)img * H * W * C;
+    for (int c = tid; c < PPIX * 4; c += 128) {
+        const int pix = c >> 2, q = c & 3;
+        const int pr = pix / PW, pc = pix - pr * PW;
+        const int gy = y0 + pr - 1, gx = x0 + pc - 1;
+        const bool in = gy >= 0 && gy < H && gx >= 0 && gx < W;
+        const bf16 *src = in ? Xi + ((long long)gy * W + gx) * C + q * 8 : Xi;
+        cp_async16(patch + q * kPlane + pix * 16, src, in ? 16 : 0);
+    }
+}
+
+struct ConvArgs {
+    const bf16 *X;
+    int nimg, H, W;
+    const bf16 *Wk;      // [cout][tap][cin]
+    const float *bias;   // [32] or null
+    int relu;            // apply max(., 0)
+    const bf16 *gate;    // optional: zero output channel n where gate[p][n] <= 0
+    bf16 *Ybf;           // BF16 output, or
+    float *Yf;           // FP32 output
+};
+
+__device__ __forceinline__ void conv_epilogue(const ConvArgs &a, const TileGeom &G, int t, uint32_t taddr, int warp,
+                                              int lane, const float *sBias) {
+    float acc[32];
+    tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16), acc);
+    const int img = t / G.per_img, r = t - img * G.per_img;
+    const int tyi = r / G.ntx, txi = r - tyi * G.ntx;
+    const int m = warp * 32 + lane, px = m & 7, py = m >> 3;
+    const int gx = txi * TXP + px, gy = tyi * TYP + py;
+    if (gx >= a.W || gy >= a.H) return;
+    const long long o = (((long long)img * a.H + gy) * a.W + gx) * C;
+#pragma unroll
+    for (int n = 0; n < 32; n++) {
+        float v = acc[n] + sBias[n];
+        if (a.relu) v = fmaxf(v, 0.f);
+        acc[n] = v;
+    }
+    if (a.gate) {
+        const uint4 *gp = reinterpret_cast<const uint4 *>(a.gate + o);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const uint4 u = gp[k];
+            const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const __nv_bfloat162 h = *reinterpret_cast<const __nv_bfloat162 *>(&w[j]);
+                if (!(__low2float(h) > 0.f)) acc[8 * k + 2 * j] = 0.f;
+                if (!(__high2float(h) > 0.f)) acc[8 * k + 2 * j + 1] = 0.f;
+            }
+        }
+    }
+    if (a.Yf) {
+        float4 *d = reinterpret_cast<float4 *>(a.Yf + o);
+#pragma unroll
+        for (int k = 0; k < 8; k++) d[k] = make_float4(acc[4 * k], acc[4 * k + 1], acc[4 * k + 2], acc[4 * k + 3]);
+    } else {
+        uint4 *d = reinterpret_cast<uint4 *>(a.Ybf + o);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            d[k] = make_uint4(pack2(acc[8 * k], acc[8 * k + 1]), pack2(acc[8 * k + 2], acc[8 * k + 3]),
+                              pack2(acc[8 * k + 4], acc[8 * k + 5]), pack2(acc[8 * k + 6], acc[8 * k + 7]));
+    }
+}
+
+__global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a) {
+    extern __shared__ unsigned char sm_raw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char *sW = sm;
+    unsigned char *sP[2] = {sm + kWBytes, sm + kWBytes + kPatch};
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + kWBytes + 2 * kPatch);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
+    __shared__ float sBias[32];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const TileGeom G = tile_geom(a.nimg, a.H, a.W);
+
+    // weights -> [tap][quarter][cout] 16-byte rows (K-major B operand)
+    for (int c = tid; c < 32 * 36; c += 128) {
+        const int n = c / 36, r = c - n * 36;  // r = tap * 4 + quarter
+        cp_async16(sW + r * 512 + n * 16, a.Wk + n * KROWS + r * 8, 16);
+    }
+    cp_async_commit();
+    if (tid < 32) sBias[tid] = a.bias ? a.bias[tid] : 0.f;
+    if (warp == 0) tmem_alloc(tslot, 64);
+    if (tid == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t id = idesc(128, 32, 0, 0);
+    const uint32_t w_u32 = smem_u32(sW);
+
+    bool failed = false;
+    int prev = -1, i = 0;
+    for (int t = blockIdx.x;; t += gridDim.x, i++) {
+        const bool have = t < G.total;
+        if (have) {
+            const int img = t / G.per_img, r = t - img * G.per_img;
+            const int tyi = r / G.ntx, txi = r - tyi * G.ntx;
+            load_patch(a.X, img, a.H, a.W, txi * TXP, tyi * TYP, sP[i & 1], tid);
+            cp_async_commit();
+        }
+        if (prev >= 0) {  // epilogue of the previous tile overlaps this tile's loads
+            const int j = i - 1;
+            const bool ok = mbar_wait(&mbar[j & 1], (j >> 1) & 1);
+            if (__syncthreads_or(!ok)) {
+                failed = true;
+                break;
+            }
+            fence_after();
+            conv_epilogue(a, G, prev, tmem + (uint32_t)((j & 1) * 32), warp, lane, sBias);
+        }
+        if (!have) break;
+        cp_async_wait_all();
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        if (tid == 0) {
+            const uint32_t p_u32 = smem_u32(sP[i & 1]);
+            const uint32_t d = tmem + (uint32_t)((i & 1) * 32);
+#pragma unroll 1
+            for (int tap = 0; tap < 9; tap++) {
+                const int dy = tap / 3, dx = tap - dy * 3;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const uint64_t da = sdesc(p_u32 + 2 * h * kPlane + (dy * PW + dx) * 16, kPlane, PW * 16);
+                    const uint64_t db = sdesc(w_u32 + (tap * 4 + 2 * h) * 512, 512, 128);
+                    mma_bf16(d, da, db, id, (tap | h) ? 1u : 0u);
+                }
+            }
+            mma_commit(&mbar[i & 1]);
+        }
+        prev = t;
+    }
+    if (failed) {
+        if (tid == 0) atomicExch(&g_corr_err, 1);
+        // the copies of this tile and the MMAs of the last issued tile may
+        // still run: wait for them once more
+        cp_async_wait_all();
+        mbar_wait(&mbar[(i - 1) & 1], ((i - 1) >> 1) & 1);
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (warp == 0) tmem_dealloc(tmem, 64);
+}
+
+// Weight (and bias) gradient, accumulated into dW[cout][288] and db[32].
+__global__ void __launch_bounds__(128, 1)
+    conv3x3_wgrad_kernel(const bf16 *__restrict__ X, const bf16 *__restrict__ dZ, int nimg, int H, int W,
+                         float *__restrict__ dW, float *__restrict__ db) {
+    extern __shared__ unsigned char sm_raw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char *sP = sm;
+    unsigned char *sZ = sm + kPatch;
+    unsigned char *sA = sZ + 4 * kZPlane;
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sA + 24 * kABlock);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const TileGeom G = tile_geom(nimg, H, W);
+
+    // rows 288..383 of A: zero, except row 288 = 1 (bias gradient); these
+    // core matrices (M groups 36..47 = block 2 groups 4..15) are never rewritten
+    for (int c = tid; c < 8 * 12 * 2 * 8; c += 128) {  // (s, group, kgroup, 16-byte row)
+        const int r = c & 7, kg = (c >> 3) & 1, g = 4 + ((c >> 4) % 12), s = c / 192;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (g == 4) v.x = 0x3F80u;  // bf16 1.0 in element 0: row 288 of this pixel
+        *reinterpret_cast<uint4 *>(sA + (s * 3 + 2) * kABlock + g * 256 + kg * 128 + r * 16) = v;
+    }
+    if (warp == 0) tmem_alloc(tslot, 128);
+    if (tid == 0) {
+        mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t id = idesc(128, 32, 1, 1);
+    const uint32_t a_u32 = smem_u32(sA), z_u32 = smem_u32(sZ);
+
+    bool failed = false;
+    int i = 0;
+    for (int t = blockIdx.x; t < G.total; t += gridDim.x, i++) {
+        const int img = t / G.per_img, r = t - img * G.per_img;
+        const int tyi = r / G.ntx, txi = r - tyi * G.ntx;
+        const int x0 = txi * TXP, y0 = tyi * TYP;
+        load_patch(X, img, H, W, x0, y0, sP, tid);
+        const bf16 *Zi = dZ + (long long)img * H * W * C;
+        for (int c = tid; c < 128 * 4; c += 128) {
+            const int m = c >> 2, q = c & 3, px = m & 7, py = m >> 3;
+            const int gx = x0 + px, gy = y0 + py;
+            const bool in = gx < W && gy < H;
+            const bf16 *src = in ? Zi + ((long long)gy * W + gx) * C + q * 8 : Zi;
+            cp_async16(sZ + q * kZPlane + m * 16, src, in ? 16 : 0);
+        }
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+        // A core matrices (s, G = tap*4 + quarter, kgroup): 8 pixels of tile
+        // row 2s + kg shifted by the tap, 8 channels each
+        for (int c = tid; c < 8 * 36 * 2; c += 128) {
+            const int s = c / 72, rem = c - s * 72, Gm = rem >> 1, kg = rem & 1;
+            const int tap = Gm >> 2, q = Gm & 3, dy = tap / 3, dx = tap - dy * 3;
+            const int py = 2 * s + kg;
+            const uint4 *src = reinterpret_cast<const uint4 *>(sP + q * kPlane + ((py + dy) * PW + dx) * 16);
+            uint4 *dst = reinterpret_cast<uint4 *>(sA + (s * 3 + (Gm >> 4)) * kABlock + (Gm & 15) * 256 + kg * 128);
+#pragma unroll
+            for (int k = 0; k < 8; k++) dst[k] = src[k];
+        }
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        if (tid == 0) {
+#pragma unroll 1
+            for (int s = 0; s < 8; s++) {
+                const uint64_t dbd = sdesc(z_u32 + s * 256, 128, kZPlane);
+#pragma unroll
+                for (int b = 0; b < 3; b++) {
+                    const uint64_t da = sdesc(a_u32 + (s * 3 + b) * kABlock, 128, 256);
+                    mma_bf16(tmem + (uint32_t)(b * 32), da, dbd, id, (i > 0 || s > 0) ? 1u : 0u);
+                }
+            }
+            mma_commit(mbar);
+        }
+        const bool ok = mbar_wait(mbar, i & 1);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            if (tid == 0) atomicExch(&g_corr_err, 1);
+            mbar_wait(mbar, i & 1);
+            break;
+        }
+        fence_after();
+    }
+    if (!failed && i > 0) {
+#pragma unroll 1
+        for (int b = 0; b < 3; b++) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * 32), v);
+            const int m = b * 128 + warp * 32 + lane;
+            if (m < KROWS) {
+#pragma unroll
+                for (int n = 0; n < 32; n++) atomicAdd(dW + n * KROWS + m, v[n]);
+            } else if (m == KROWS && db) {
+#pragma unroll
+                for (int n = 0; n < 32; n++) atomicAdd(db + n, v[n]);
+            }
+        }
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (warp == 0) tmem_dealloc(tmem, 128);
+}
+
+// ---------------------------------------------------------------- training
+// Feature scales (metres per unit)
+constexpr float kSh = 2.0f;    // maximum depth
+constexpr float kSb = 0.05f;   // bed change
+constexpr float kSH = 50.0f;   // bathymetry
+constexpr float kSdH = 2.0f;   // sub-grid bathymetry detail
+
+// bilinear sample of a coarse [hc][wc] plane at fine cell (x, y), factor f,
+// cell-centred, clamped at the edges
+__device__ __forceinline__ float up_bilinear(const float *__restrict__ p, int hc, int wc, int f, int x, int y) {
+    const float cx = (x + 0.5f) / f - 0.5f, cy = (y + 0.5f) / f - 0.5f;
+    const float fx = fminf(fmaxf(cx, 0.f), (float)(wc - 1)), fy = fminf(fmaxf(cy, 0.f), (float)(hc - 1));
+    const int x0 = min((int)fx, wc - 1), y0 = min((int)fy, hc - 1);
+    const int x1 = min(x0 + 1, wc - 1), y1 = min(y0 + 1, hc - 1);
+    const float ax = fx - x0, ay = fy - y0;
+    const float a = p[y0 * wc + x0], b = p[y0 * wc + x1], c = p[y1 * wc + x0], d = p[y1 * wc + x1];
+    return (1.f - ay) * ((1.f - ax) * a + ax * b) + ay * ((1.f - ax) * c + ax * d);
+}
+
+// Builds the 32-channel BF16 input of sample idx[b] and, when targets are
+// requested, the normalised residual targets T[b][p][2].
+//   coarse: [nsamples][3][hc*wc] = maximum depth, bed change, bathymetry H
+//   fineT:  [nsamples][2][H*W]   = maximum depth, bed change (or null)
+__global__ void features_kernel(const int *__restrict__ idx, int nb, const float *__restrict__ coarse,
+                                const float *__restrict__ fineT, const float *__restrict__ Hf, int H, int W, int hc,
+                                int wc, int f, bf16 *__restrict__ X0, float *__restrict__ T, float *__restrict__ base) {
+    const long long npix = (long long)H * W;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nb * npix;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(g / npix);
+        const long long p = g - (long long)b * npix;
+        const int y = (int)(p / W), x = (int)(p - (long long)y * W);
+        const int s = idx[b];
+        const float *cs = coarse + (long long)s * 3 * hc * wc;
+        const float hm = up_bilinear(cs, hc, wc, f, x, y);
+        const float dbv = up_bilinear(cs + hc * wc, hc, wc, f, x, y);
+        const float Hc = up_bilinear(cs + 2 * hc * wc, hc, wc, f, x, y);
+        const float Hfine = Hf[p];
+        const int xi = min(x / f, wc - 1), yi = min(y / f, hc - 1);  // coarse cell containing the fine cell
+        const float wet = cs[yi * wc + xi] > 0.f ? 1.f : 0.f;
+        const float v[8] = {hm / kSh, dbv / kSb, Hfine / kSH, (Hfine - Hc) / kSdH, wet, 0.f, 0.f, 0.f};
+        uint4 *d = reinterpret_cast<uint4 *>(X0 + g * C);
+        d[0] = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
+        d[1] = d[2] = d[3] = make_uint4(0, 0, 0, 0);
+        if (base) {
+            base[g * 2] = hm;
+            base[g * 2 + 1] = dbv;
+        }
+        if (T && fineT) {
+            const float *ft = fineT + (long long)s * 2 * npix;
+            T[g * 2] = (ft[p] - hm) / kSh;
+            T[g * 2 + 1] = (ft[npix + p] - dbv) / kSb;
+        }
+    }
+}
+
+// Mean-square loss over the 2 output channels; dY = d(loss)/d(output) in
+// BF16 (channels 2..31 zero); loss sum accumulated in FP64.
+__global__ void loss_kernel(const float *__restrict__ Y, const float *__restrict__ T, long long npix,
+                            bf16 *__restrict__ dY, double *__restrict__ loss) {
+    __shared__ double sred[32];
+    const float scale = 1.f / (float)npix;  // d/dy of sum(d^2) / (2 npix)
+    double acc = 0.0;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
+         p += (long long)gridDim.x * blockDim.x) {
+        const float d0 = Y[p * C] - T[p * 2], d1 = Y[p * C + 1] - T[p * 2 + 1];
+        acc += (double)d0 * d0 + (double)d1 * d1;
+        uint4 *g = reinterpret_cast<uint4 *>(dY + p * C);
+        g[0] = make_uint4(pack2(scale * d0, scale * d1), 0, 0, 0);
+        g[1] = g[2] = g[3] = make_uint4(0, 0, 0, 0);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += sred[w];
+        atomicAdd(loss, s);
+    }
+}
+
+// Adam on the FP32 master weights and biases of all layers; refreshes the
+// BF16 weights and their tap-flipped transpose (the input-gradient weights:
+// Wt[cin][8 - tap][cout] = W[cout][tap][cin]).
+__global__ void adam_kernel(float *__restrict__ Wm, float *__restrict__ mW, float *__restrict__ vW,
+                            const float *__restrict__ gW, float *__restrict__ Bm, float *__restrict__ mB,
+                            float *__restrict__ vB, const float *__restrict__ gB, int nlayers, float lr, float b1,
+                            float b2, float c1, float c2, float eps, bf16 *__restrict__ Wbf, bf16 *__restrict__ Wt) {
+    const int nw = nlayers * 32 * KROWS;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nw + nlayers * 32; k += gridDim.x * blockDim.x) {
+        if (k < nw) {
+            const float g = gW[k];
+            const float m = b1 * mW[k] + (1.f - b1) * g, v = b2 * vW[k] + (1.f - b2) * g * g;
+            mW[k] = m;
+            vW[k] = v;
+            const float w = Wm[k] - lr * (m / c1) / (sqrtf(v / c2) + eps);
+            Wm[k] = w;
+            const int l = k / (32 * KROWS), r = k - l * 32 * KROWS, co = r / KROWS, kk = r - co * KROWS;
+            const int tap = kk / 32, ci = kk - tap * 32;
+            Wbf[k] = __float2bfloat16_rn(w);
+            Wt[l * 32 * KROWS + ci * KROWS + (8 - tap) * 32 + co] = __float2bfloat16_rn(w);
+        } else {
+            const int j = k - nw;
+            const float g = gB[j];
+            const float m = b1 * mB[j] + (1.f - b1) * g, v = b2 * vB[j] + (1.f - b2) * g * g;
+            mB[j] = m;
+            vB[j] = v;
+            Bm[j] -= lr * (m / c1) / (sqrtf(v / c2) + eps);
+        }
+    }
+}
+
+// corrected fields: base + scale * output channel
+__global__ void apply_kernel(const float *__restrict__ Y, const float *__restrict__ base, long long npix,
+                             float *__restrict__ out_h, float *__restrict__ out_b) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
+         p += (long long)gridDim.x * blockDim.x) {
+        out_h[p] = base[p * 2] + kSh * Y[p * C];
+        out_b[p] = base[p * 2 + 1] + kSb * Y[p * C + 1];
+    }
+}
+
+cudaError_t prepare() {
+    static bool done = false;
+    if (done) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(conv3x3_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(conv3x3_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem);
+    if (e == cudaSuccess) done = true;
+    return e;
+}
+
+int num_sms() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+    }
+    return n;
+}
+
+cudaError_t conv_launch(const ConvArgs &a, cudaStream_t st) {
+    cudaError_t e = prepare();
+    if (e != cudaSuccess) return e;
+    const TileGeom G = tile_geom(a.nimg, a.H, a.W);
+    const int ctas = std::min(G.total, 4 * num_sms());
+    conv3x3_fwd_kernel<<<ctas, 128, kFwdSmem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t wgrad_launch(const bf16 *X, const bf16 *dZ, int nimg, int H, int W, float *dW, float *db, cudaStream_t st) {
+    cudaError_t e = prepare();
+    if (e != cudaSuccess) return e;
+    const TileGeom G = tile_geom(nimg, H, W);
+    const int ctas = std::min(G.total, num_sms());
+    conv3x3_wgrad_kernel<<<ctas, 128, kWgSmem, st>>>(X, dZ, nimg, H, W, dW, db);
+    return cudaGetLastError();
+}
+
+}  // namespace corr
+}  // namespace tsu
+
+using namespace tsu::corr;
+
+// ------------------------------------------------------------ the corrector
+struct TsuCorrector {
+    int device = 0;
+    int H = 0, W = 0, f = 1, hc = 0, wc = 0, max_batch = 0;
+    static constexpr int L = 6;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    // parameters
+    float *Wm = nullptr, *mW = nullptr, *vW = nullptr, *gW = nullptr;  // [L][32][288]
+    float *Bm = nullptr, *mB = nullptr, *vB = nullptr, *gB = nullptr;  // [L][32]
+    bf16 *Wbf = nullptr, *Wt = nullptr;
+    long adam_t = 0;
+    // activations [max_batch][H][W][32]: act[0] = features, act[l] = output of layer l-1
+    bf16 *act[L] = {};
+    float *Yout = nullptr;
+    bf16 *g0 = nullptr, *g1 = nullptr;
+    float *T = nullptr, *base = nullptr;  // [max_batch][H][W][2]
+    int *d_idx = nullptr;
+    double *d_loss = nullptr;
+    // data set
+    float *Hf = nullptr;                       // fine bathymetry
+    float *coarse = nullptr, *fine = nullptr;  // [n][3][hc*wc], [n][2][H*W]
+    int nsamples = 0, cap = 0;
+    double last_ms = 0.0;
+    long last_convs = 0;
+};
+
+namespace {
+thread_local char g_corr_msg[256] = "";
+#define CCK(call)                                                                                \
+    do {                                                                                         \
+        cudaError_t _e = (call);                                                                 \
+        if (_e != cudaSuccess) {                                                                 \
+            snprintf(g_corr_msg, sizeof(g_corr_msg), "%s: %s", #call, cudaGetErrorString(_e));   \
+            return _e == cudaErrorMemoryAllocation ? TSU_ERR_GPU_OOM : TSU_ERR_CUDA;             \
+        }                                                                                        \
+    } while (0)
+
+uint64_t splitmix(uint64_t &s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+double uniform01(uint64_t &s) { return (double)(splitmix(s) >> 11) * (1.0 / 9007199254740992.0); }
+
+void free_all(TsuCorrector *c) {
+    float *fp[] = {c->Wm, c->mW, c->vW, c->gW, c->Bm, c->mB, c->vB, c->gB, c->Yout, c->T, c->base, c->Hf, c->coarse, c->fine};
+    for (float *p : fp) cudaFree(p);
+    cudaFree(c->Wbf);
+    cudaFree(c->Wt);
+    for (bf16 *p : c->act) cudaFree(p);
+    cudaFree(c->g0);
+    cudaFree(c->g1);
+    cudaFree(c->d_idx);
+    cudaFree(c->d_loss);
+    if (c->e0) cudaEventDestroy(c->e0);
+    if (c->e1) cudaEventDestroy(c->e1);
+    if (c->st) cudaStreamDestroy(c->st);
+}
+
+int upload_weights(TsuCorrector *c, const float *W, const float *B) {
+    const int L = TsuCorrector::L;
+    const size_t nw = (size_t)L * 32 * KROWS;
+    std::vector<bf16> wb(nw), wt(nw);
+    for (int l = 0; l < L; l++)
+        for (int co = 0; co < 32; co++)
+            for (int kk = 0; kk < KROWS; kk++) {
+                const size_t k = ((size_t)l * 32 + co) * KROWS + kk;
+                const int tap = kk / 32, ci = kk % 32;
+                const bf16 v = __float2bfloat16_rn(W[k]);
+                wb[k] = v;
+                wt[(size_t)l * 32 * KROWS + ci * KROWS + (8 - tap) * 32 + co] = v;
+            }
+    CCK(cudaMemcpyAsync(c->Wm, W, nw * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    CCK(cudaMemcpyAsync(c->Bm, B, (size_t)L * 32 * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    CCK(cudaMemcpyAsync(c->Wbf, wb.data(), nw * sizeof(bf16), cudaMemcpyHostToDevice, c->st));
+    CCK(cudaMemcpyAsync(c->Wt, wt.data(), nw * sizeof(bf16), cudaMemcpyHostToDevice, c->st));
+    CCK(cudaMemsetAsync(c->mW, 0, nw * sizeof(float), c->st));
+    CCK(cudaMemsetAsync(c->vW, 0, nw * sizeof(float), c->st));
+    CCK(cudaMemsetAsync(c->mB, 0, (size_t)L * 32 * sizeof(float), c->st));
+    CCK(cudaMemsetAsync(c->vB, 0, (size_t)L * 32 * sizeof(float), c->st));
+    CCK(cudaStreamSynchronize(c->st));
+    c->adam_t = 0;
+    return TSU_OK;
+}
+
+int check_kernel_flag() {
+    int flag = 0;
+    CCK(cudaMemcpyFromSymbol(&flag, g_corr_err, sizeof(int)));
+    if (flag) {
+        snprintf(g_corr_msg, sizeof(g_corr_msg), "corrector: a tensor-core wait expired");
+        int z = 0;
+        cudaMemcpyToSymbol(g_corr_err, &z, sizeof(int));
+        return TSU_ERR_CUDA;
+    }
+    return TSU_OK;
+}
+
+// forward pass of `nb` images already in act[0]; FP32 output in Yout
+int forward(TsuCorrector *c, int nb) {
+    const int L = TsuCorrector::L;
+    for (int l = 0; l < L; l++) {
+        ConvArgs a;
+        a.X = c->act[l];
+        a.nimg = nb;
+        a.H = c->H;
+        a.W = c->W;
+        a.Wk = c->Wbf + (size_t)l * 32 * KROWS;
+        a.bias = c->Bm + l * 32;
+        a.relu = (l < L - 1);
+        a.gate = nullptr;
+        a.Ybf = (l < L - 1) ? c->act[l + 1] : nullptr;
+        a.Yf = (l < L - 1) ? nullptr : c->Yout;
+        CCK(conv_launch(a, c->st));
+    }
+    return TSU_OK;
+}
+
+int load_batch(TsuCorrector *c, const int *idx, int nb, bool targets) {
+    CCK(cudaMemcpyAsync(c->d_idx, idx, nb * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    features_kernel<<<4 * num_sms(), 256, 0, c->st>>>(c->d_idx, nb, c->coarse, targets ? c->fine : nullptr, c->Hf, c->H,
+                                                      c->W, c->hc, c->wc, c->f, c->act[0], targets ? c->T : nullptr,
+                                                      c->base);
+    CCK(cudaGetLastError());
+    return TSU_OK;
+}
+}  // namespace
+
+extern "C" int tsu_corr_create(TsuCorrector **out, int ny, int nx, int factor, int max_batch, unsigned long long seed,
+                               int device) {
+    if (!out || ny < 1 || nx < 1 || factor < 1 || ny % factor || nx % factor || max_batch < 1) return TSU_ERR_INVALID;
+    *out = nullptr;
+    TsuCorrector *c = new (std::nothrow) TsuCorrector();
+    if (!c) return TSU_ERR_HOST_OOM;
+    c->device = device;
+    c->H = ny;
+    c->W = nx;
+    c->f = factor;
+    c->hc = ny / factor;
+    c->wc = nx / factor;
+    c->max_batch = max_batch;
+    const int L = TsuCorrector::L;
+    const size_t nw = (size_t)L * 32 * KROWS, nbias = (size_t)L * 32;
+    const size_t npix = (size_t)max_batch * ny * nx;
+    cudaError_t e = cudaSetDevice(device);
+#define CAL(p, bytes) \
+    if (e == cudaSuccess) e = cudaMalloc((void **)&(p), (bytes))
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->e1);
+    CAL(c->Wm, nw * 4);
+    CAL(c->mW, nw * 4);
+    CAL(c->vW, nw * 4);
+    CAL(c->gW, nw * 4);
+    CAL(c->Bm, nbias * 4);
+    CAL(c->mB, nbias * 4);
+    CAL(c->vB, nbias * 4);
+    CAL(c->gB, nbias * 4);
+    CAL(c->Wbf, nw * 2);
+    CAL(c->Wt, nw * 2);
+    for (int l = 0; l < L; l++) CAL(c->act[l], npix * C * 2);
+    CAL(c->Yout, npix * C * 4);
+    CAL(c->g0, npix * C * 2);
+    CAL(c->g1, npix * C * 2);
+    CAL(c->T, npix * 2 * 4);
+    CAL(c->base, npix * 2 * 4);
+    CAL(c->d_idx, (size_t)max_batch * 4);
+    CAL(c->d_loss, 8);
+    CAL(c->Hf, (size_t)ny * nx * 4);
+#undef CAL
+    if (e == cudaSuccess) e = prepare();
+    if (e != cudaSuccess) {
+        snprintf(g_corr_msg, sizeof(g_corr_msg), "tsu_corr_create: %s", cudaGetErrorString(e));
+        free_all(c);
+        delete c;
+        return e == cudaErrorMemoryAllocation ? TSU_ERR_GPU_OOM : TSU_ERR_CUDA;
+    }
+    // He-normal initialisation (SplitMix64 + Box-Muller); the last layer is
+    // zero, so the untrained corrector returns the interpolated coarse fields
+    std::vector<float> W(nw, 0.f), B(nbias, 0.f);
+    uint64_t s = seed;
+    const double sd = std::sqrt(2.0 / (9.0 * 32.0));
+    for (int l = 0; l < L - 1; l++)
+        for (size_t k = 0; k < (size_t)32 * KROWS; k++) {
+            const double u1 = uniform01(s), u2 = uniform01(s);
+            W[(size_t)l * 32 * KROWS + k] = (float)(sd * std::sqrt(-2.0 * std::log1p(-u1)) * std::cos(2.0 * M_PI * u2));
+        }
+    int rc = upload_weights(c, W.data(), B.data());
+    if (rc) {
+        free_all(c);
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return TSU_OK;
+}
+
+extern "C" int tsu_corr_destroy(TsuCorrector *c) {
+    if (!c) return TSU_OK;
+    cudaSetDevice(c->device);
+    if (c->st) cudaStreamSynchronize(c->st);
+    free_all(c);
+    delete c;
+    return TSU_OK;
+}
+
+extern "C" int tsu_corr_set_site(TsuCorrector *c, const float *fine_H) {
+    if (!c || !fine_H) return TSU_ERR_INVALID;
+    CCK(cudaSetDevice(c->device));
+    CCK(cudaMemcpyAsync(c->Hf, fine_H, (size_t)c->H * c->W * 4, cudaMemcpyHostToDevice, c->st));
+    CCK(cudaStreamSynchronize(c->st));
+    return TSU_OK;
+}
+
+extern "C" int tsu_corr_add_samples(TsuCorrector *c, int n, const float *coarse, const float *fine) {
+    if (!c || n < 1 || !coarse) return TSU_ERR_INVALID;
+    CCK(cudaSetDevice(c->device));
+    const size_t cs = (size_t)3 * c->hc * c->wc, fs = (size_t)2 * c->H * c->W;
+    if (c->nsamples + n > c->cap) {
+        const int ncap = std::max(c->nsamples + n, 2 * c->cap);
+        float *nc = nullptr, *nf = nullptr;
+        CCK(cudaMalloc((void **)&nc, ncap * cs * 4));
+        if (cudaMalloc((void **)&nf, ncap * fs * 4) != cudaSuccess) {
+            cudaFree(nc);
+            snprintf(g_corr_msg, sizeof(g_corr_msg), "tsu_corr_add_samples: out of device memory");
+            return TSU_ERR_GPU_OOM;
+        }
+        if (c->nsamples) {
+            CCK(cudaMemcpyAsync(nc, c->coarse, c->nsamples * cs * 4, cudaMemcpyDeviceToDevice, c->st));
+            CCK(cudaMemcpyAsync(nf, c->fine, c->nsamples * fs * 4, cudaMemcpyDeviceToDevice, c->st));
+        }
+        CCK(cudaStreamSynchronize(c->st));
+        cudaFree(c->coarse);
+        cudaFree(c->fine);
+        c->coarse = nc;
+        c->fine = nf;
+        c->cap = ncap;
+    }
+    CCK(cudaMemcpyAsync(c->coarse + c->nsamples * cs, coarse, n * cs * 4, cudaMemcpyHostToDevice, c->st));
+    if (fine)
+        CCK(cudaMemcpyAsync(c->fine + c->nsamples * fs, fine, n * fs * 4, cudaMemcpyHostToDevice, c->st));
+    else
+        CCK(cudaMemsetAsync(c->fine + c->nsamples * fs, 0, n * fs * 4, c->st));
+    CCK(cudaStreamSynchronize(c->st));
+    c->nsamples += n;
+    return TSU_OK;
+}
+
+extern "C" int tsu_corr_num_samples(TsuCorrector *c, int *n) {
+    if (!c || !n) return TSU_ERR_INVALID;
+    *n = c->nsamples;
+    return TSU_OK;
+}
+
+extern "C" int tsu_corr_get_weights(TsuCorrector *c, float *W, float *B) {
+    if (!c || !W || !B) return TSU_ERR_INVALID;
+    CCK(cudaSetDevice(c->device));
+    CCK(cudaMemcpyAsync(W, c->Wm, (size_t)TsuCorrector::L * 32 * KROWS * 4, cudaMemcpyDeviceToHost, c->st));
+    CCK(cudaMemcpyAsync(B, c->Bm, (size_t)TsuCorrector::L * 32 * 4, cudaMemcpyDeviceToHost, c->st));
+    CCK(cudaStreamSynchronize(c->st));
+    return TSU_OK;
+}
+
+extern "C" int tsu_corr_set_weights(TsuCorrector *c, const float *W, const float *B) {
+    if (!c || !W || !B) return TSU_ERR_INVALID;
+    CCK(cudaSetDevice(c->device));
+    return upload_weights(c, W, B);
+}
+
+// `iters` Adam steps on mini-batches drawn (seeded) from samples [0, ntrain)
+extern "C" int tsu_corr_train(TsuCorrector *c, int ntrain, int iters, int batch, float lr, unsigned long long seed,
+                              float *loss) {
+    if (!c || ntrain < 1 || ntrain > c->nsamples || iters < 0 || batch < 1 || batch > c->max_batch)
+        return TSU_ERR_INVALID;
+    CCK(cudaSetDevice(c->device));
+    const int L = TsuCorrector::L;
+    const size_t nw = (size_t)L * 32 * KROWS;
+    const long long npix = (long long)batch * c->H * c->W;
+    uint64_t s = seed;
+    std::vector<int> idx(batch);
+    double *h_loss = nullptr;
+    CCK(cudaMallocHost((void **)&h_loss, sizeof(double) * std::max(iters, 1)));
+    int rc = TSU_OK;
+    cudaError_t e = cudaEventRecord(c->e0, c->st);
+    for (int it = 0; it < iters && !rc && e == cudaSuccess; it++) {
+        for (int b = 0; b < batch; b++) idx[b] = (int)(splitmix(s) % (uint64_t)ntrain);
+        rc = load_batch(c, idx.data(), batch, true);
+        if (!rc) rc = forward(c, batch);
+        if (rc) break;
+        e = cudaMemsetAsync(c->d_loss, 0, 8, c->st);
+        if (e != cudaSuccess) break;
+        loss_kernel<<<4 * num_sms(), 256, 0, c->st>>>(c->Yout, c->T, npix, c->g0, c->d_loss);
+        if ((e = cudaGetLastError()) != cudaSuccess) break;
+        if ((e = cudaMemcpyAsync(h_loss + it, c->d_loss, 8, cudaMemcpyDeviceToHost, c->st)) != cudaSuccess) break;
+        if ((e = cudaMemsetAsync(c->gW, 0, nw * 4, c->st)) != cudaSuccess) break;
+        if ((e = cudaMemsetAsync(c->gB, 0, (size_t)L * 32 * 4, c->st)) != cudaSuccess) break;
+        bf16 *dZ = c->g0, *dX = c->g1;
+        for (int l = L - 1; l >= 0 && e == cudaSuccess; l--) {
+            e = wgrad_launch(c->act[l], dZ, batch, c->H, c->W, c->gW + (size_t)l * 32 * KROWS, c->gB + l * 32, c->st);
+            if (e == cudaSuccess && l > 0) {  // dZ_{l-1} = conv(dZ_l, flipped W_l), zero where act[l] <= 0
+                ConvArgs a;
+                a.X = dZ;
+                a.nimg = batch;
+                a.H = c->H;
+                a.W = c->W;
+                a.Wk = c->Wt + (size_t)l * 32 * KROWS;
+                a.bias = nullptr;
+                a.relu = 0;
+                a.gate = c->act[l];
+                a.Ybf = dX;
+                a.Yf = nullptr;
+                e = conv_launch(a, c->st);
+                std::swap(dZ, dX);
+            }
+        }
+        if (e != cudaSuccess) break;
+        c->adam_t++;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f - powf(b1, (float)c->adam_t), c2 = 1.f - powf(b2, (float)c->adam_t);
+        adam_kernel<<<(int)((nw + 255) / 256), 256, 0, c->st>>>(c->Wm, c->mW, c->vW, c->gW, c->Bm, c->mB, c->vB, c->gB,
+                                                              L, lr, b1, b2, c1, c2, 1e-8f, c->Wbf, c->Wt);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && !rc) e = cudaEventRecord(c->e1, c->st);
+    if (e == cudaSuccess && !rc) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess && !rc) {
+        snprintf(g_corr_msg, sizeof(g_corr_msg), "tsu_corr_train: %s", cudaGetErrorString(e));
+        rc = TSU_ERR_CUDA;
+    }
+    if (!rc) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->e0, c->e1);
+        c->last_ms = ms;
+        c->last_convs = (long)iters * (3 * L - 1);
+        if (loss)
+            for (int it = 0; it < iters; it++) loss[it] = (float)(h_loss[it] / (2.0 * (double)npix));
+    }
+    cudaFreeHost(h_loss);
+    if (rc) return rc;
+    return check_kernel_flag();
+}
+
+// corrected (and interpolated baseline) fine fields of samples
+// [first, first + n): out_* are [n][H][W]; base_* may be null
+extern "C" int tsu_corr_predict(TsuCorrector *c, int first, int n, float *out_hmax, float *out_db, float *base_hmax,
+                                float *base_db) {
+    if (!c || first < 0 || n < 1 || first + n > c->nsamples || !out_hmax || !out_db) return TSU_ERR_INVALID;
+    CCK(cudaSetDevice(c->device));
+    const size_t np = (size_t)c->H * c->W;
+    float *d_out = nullptr;
+    CCK(cudaMalloc((void **)&d_out, 2 * np * 4));
+    std::vector<float> bb(2 * np);
+    int rc = TSU_OK;
+    for (int k = 0; k < n && !rc; k++) {
+        const int s = first + k;
+        rc = load_batch(c, &s, 1, false);
+        if (!rc) rc = forward(c, 1);
+        if (rc) break;
+        apply_kernel<<<2 * num_sms(), 256, 0, c->st>>>(c->Yout, c->base, (long long)np, d_out, d_out + np);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(out_hmax + k * np, d_out, np * 4, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+            cudaMemcpyAsync(out_db + k * np, d_out + np, np * 4, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+            cudaMemcpyAsync(bb.data(), c->base, 2 * np * 4, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+            cudaStreamSynchronize(c->st) != cudaSuccess) {
+            snprintf(g_corr_msg, sizeof(g_corr_msg), "tsu_corr_predict: CUDA error");
+            rc = TSU_ERR_CUDA;
+            break;
+        }
+        for (size_t p = 0; p < np; p++) {
+            if (base_hmax) base_hmax[k * np + p] = bb[2 * p];
+            if (base_db) base_db[k * np + p] = bb[2 * p + 1];
+        }
+    }
+    cudaFree(d_out);
+    if (rc) return rc;
+    return check_kernel_flag();
+}
+
+// times `iters` forward convolutions of one layer over `nimg` images of the
+// first sample's features: device ms per convolution and TFLOP/s
+// (2 x pixels x 288 x 32 FLOPs per convolution)
+extern "C" int tsu_corr_bench_conv(TsuCorrector *c, int nimg, int iters, double *ms_per_conv, double *tflops) {
+    if (!c || nimg < 1 || nimg > c->max_batch || iters < 1 || c->nsamples < 1) return TSU_ERR_INVALID;
+    CCK(cudaSetDevice(c->device));
+    std::vector<int> idx(nimg, 0);
+    int rc = load_batch(c, idx.data(), nimg, false);
+    if (rc) return rc;
+    ConvArgs a;
+    a.X = c->act[0];
+    a.nimg = nimg;
+    a.H = c->H;
+    a.W = c->W;
+    a.Wk = c->Wbf;
+    a.bias = c->Bm;
+    a.relu = 1;
+    a.gate = nullptr;
+    a.Ybf = c->act[1];
+    a.Yf = nullptr;
+    for (int k = 0; k < 3; k++) CCK(conv_launch(a, c->st));
+    CCK(cudaEventRecord(c->e0, c->st));
+    for (int k = 0; k < iters; k++) CCK(conv_launch(a, c->st));
+    CCK(cudaEventRecord(c->e1, c->st));
+    CCK(cudaEventSynchronize(c->e1));
+    float ms = 0.f;
+    CCK(cudaEventElapsedTime(&ms, c->e0, c->e1));
+    const double per = ms / iters;
+    if (ms_per_conv) *ms_per_conv = per;
+    if (tflops) *tflops = 2.0 * nimg * (double)c->H * c->W * KROWS * 32 / (per * 1e-3) / 1e12;
+    return check_kernel_flag();
+}
+
+extern "C" int tsu_corr_last_train_ms(TsuCorrector *c, double *ms, long *convs) {
+    if (!c || !ms) return TSU_ERR_INVALID;
+    *ms = c->last_ms;
+    if (convs) *convs = c->last_convs;
+    return TSU_OK;
+}
+
+// ---- raw kernels on caller-owned device buffers (stream: a cudaStream_t or null)
+extern "C" int tsu_corr_conv3x3(const void *X, int nimg, int H, int W, const void *Wk, const float *bias, int relu,
+                                const void *gate, void *Ybf, float *Yf, void *stream) {
+    if (!X || !Wk || nimg < 1 || H < 1 || W < 1 || (!Ybf && !Yf)) return TSU_ERR_INVALID;
+    ConvArgs a;
+    a.X = static_cast<const bf16 *>(X);
+    a.nimg = nimg;
+    a.H = H;
+    a.W = W;
+    a.Wk = static_cast<const bf16 *>(Wk);
+    a.bias = bias;
+    a.relu = relu;
+    a.gate = static_cast<const bf16 *>(gate);
+    a.Ybf = static_cast<bf16 *>(Ybf);
+    a.Yf = Yf;
+    CCK(conv_launch(a, static_cast<cudaStream_t>(stream)));
+    return TSU_OK;
+}
+
+extern "C" int tsu_corr_conv3x3_wgrad(const void *X, const void *dZ, int nimg, int H, int W, float *dW, float *db,
+                                      void *stream) {
+    if (!X || !dZ || !dW || nimg < 1 || H < 1 || W < 1) return TSU_ERR_INVALID;
+    CCK(wgrad_launch(static_cast<const bf16 *>(X), static_cast<const bf16 *>(dZ), nimg, H, W, dW, db,
+                     static_cast<cudaStream_t>(stream)));
+    return TSU_OK;
+}
+
+// synchronises the device and reports (and clears) an expired kernel wait
+extern "C" int tsu_corr_status(void) {
+    CCK(cudaDeviceSynchronize());
+    return check_kernel_flag();
+}
+
+extern "C" const char *tsu_corr_last_error(void) { return g_corr_msg; }

@@ -46,6 +46,7 @@ __global__ void set_scal_kernel(double *scal, int i, double v) { scal[i] = v; }
 }  // namespace
 
 const char *tsu_last_error_detail() { return g_err; }
+void tsu_set_error_detail(const char *text) { snprintf(g_err, sizeof(g_err), "%s", text); }
 
 static int validate(const SimParams *p, const TsuSwitches *sw) {
     if (!p || !sw) return TSU_ERR_INVALID;

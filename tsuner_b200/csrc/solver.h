@@ -44,3 +44,5 @@ struct TsuSolver {
 };
 
 const char *tsu_last_error_detail();
+// sets the detail text that tsu_last_error() returns on this thread
+void tsu_set_error_detail(const char *text);

@@ -1,35 +1,37 @@
-// stage32.cu -- FP32 precision form: one fused kernel per RK stage.
+// stage32.cu -- FP32 precision form: one fused kernel per RK stage, for a
+// single grid (stage32_kernel) and for a batched ensemble of grids of uneven
+// size in one persistent launch (ens32_kernel).
 //
 // Same pipeline as stage64.cu (tile + 2-cell halo in shared memory, faces,
 // each edge once, cell update, on-device dt/extrema), on the FP32 state
-// planes (z = eta - eta0, qx, qy, H, hc) with the FP64 islands of
+// planes (z = eta - eta0, H, qx, qy, hc) with the FP64 islands of
 // physics32.cuh.  The last stage also accumulates the FP64 global sums of
 // water volume sum(h) and sediment volume sum(H + hc) (per-CTA partials,
-// reduced by the last CTA in a fixed order, so the sums are deterministic).
+// reduced by the last CTA of the grid in a fixed order: deterministic).
 // Algorithmic bytes per cell-step: 5 planes x 4 B read+write per stage
 // (stage 2 also reads U^n) = 100 B, mask 2 B, extrema 3 x 8 B = 126 B.
 #include <cuda_runtime.h>
+
+#include <cstdlib>
 
 #include "physics32.cuh"
 #include "stage32.h"
 
 namespace tsu {
 
-namespace {
-constexpr int TX = 32, TY = 8, NT = TX * TY;
-constexpr int LX = TX + 4, LY = TY + 4, PS = LX * LY;
-constexpr int FXW = TX + 2, FYH = TY + 2;
-// per loaded cell: z, H, qx, qy, hc (loaded) + h, ux, uy, c (derived)
-constexpr int kSV = 9 * PS;
-constexpr int kFlux = 20 * TY * TX;
-constexpr int kRegA = kSV > kFlux ? kSV : kFlux;
-constexpr int kFx = 12 * TY * FXW, kFy = 12 * FYH * TX;  // 2 faces x 6 floats
-constexpr int kDeta = 2 * TY * TX;
-constexpr int kFloats = kRegA + kFx + kFy + kDeta;
-constexpr int kWarps = NT / 32;
-}  // namespace
-
-size_t stage32_smem_bytes() { return sizeof(float) * kFloats + sizeof(double) * 3 * kWarps + PS + 64; }
+template <int TX_, int TY_>
+struct T32 {
+    static constexpr int TX = TX_, TY = TY_, NT = TX * TY;
+    static constexpr int LX = TX + 4, LY = TY + 4, PS = LX * LY;
+    static constexpr int FXW = TX + 2, FYH = TY + 2;
+    // per loaded cell: z, H, qx, qy, hc (loaded) + h, ux, uy, c (derived)
+    static constexpr int kSV = 9 * PS, kFlux = 20 * TY * TX;
+    static constexpr int kRegA = kSV > kFlux ? kSV : kFlux;
+    static constexpr int kFx = 12 * TY * FXW, kFy = 12 * FYH * TX;  // 2 faces x 6 floats
+    static constexpr int kDeta = 2 * TY * TX, kWarps = NT / 32;
+    static constexpr int kFloats = kRegA + kFx + kFy + kDeta;
+    static constexpr size_t smem() { return sizeof(float) * kFloats + sizeof(double) * 3 * kWarps + PS + 64; }
+};
 
 __device__ __forceinline__ int wrap_clamp32(int g, int n, bool periodic) {
     if (periodic) {
@@ -59,6 +61,7 @@ __device__ __forceinline__ Face32 get_face(const float *base, int stride) {
 }
 
 // smem cell planes: 0 z, 1 H, 2 qx, 3 qy, 4 hc, 5 h, 6 ux, 7 uy, 8 c
+template <int PS>
 __device__ __forceinline__ void recon32(const Phys32 &P, const float *s, int c, int l, int r, Face32 &fm, Face32 &fp,
                                         float &deta) {
     const float hi = s[5 * PS + c], hl = s[5 * PS + l], hr = s[5 * PS + r];
@@ -113,27 +116,35 @@ __device__ __forceinline__ void recon32(const Phys32 &P, const float *s, int c, 
     filter32(fp, P.eta0);
 }
 
-template <int ORDER, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
-    extern __shared__ __align__(16) float smem32[];
-    const Phys32 &P = A.phys;
+// One RK stage on tile (bx, by) of grid A.  blin / nb: linear index of the
+// tile and number of tiles of this grid (for the end-of-step reduction).
+// P: the grid's physical parameters (A.phys, or the ensemble's shared
+// parameters with this member's grid fields).
+template <int TX, int TY, int ORDER, bool FIRST, bool LAST>
+__device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 &P, int bx, int by, unsigned blin,
+                                             unsigned nb, float *smem32) {
+    using T = T32<TX, TY>;
+    constexpr int NT = T::NT, LX = T::LX, PS = T::PS, FXW = T::FXW, FYH = T::FYH, kWarps = T::kWarps;
     float *sV = smem32;
     float *sFlux = smem32;
-    float *sFx = smem32 + kRegA;
-    float *sFy = sFx + kFx;
-    float *sDeta = sFy + kFy;
-    double *sRed = reinterpret_cast<double *>(sDeta + kDeta);  // [3][kWarps]
+    float *sFx = smem32 + T::kRegA;
+    float *sFy = sFx + T::kFx;
+    float *sDeta = sFy + T::kFy;
+    double *sRed = reinterpret_cast<double *>(sDeta + T::kDeta);  // [3][kWarps]
     unsigned char *sM = reinterpret_cast<unsigned char *>(sRed + 3 * kWarps);
     __shared__ int sLast;
 
-    const double t = A.scal[SC_T];
-    if (!(t < A.scal[SC_TEND])) return;
-    const double dtd = A.scal[SC_DT];
+    // Global memory is accessed through explicit global-space loads and
+    // stores: in the ensemble the buffer pointers come from a descriptor in
+    // shared memory, and generic accesses through them are slower.
+    const double t = __ldcg(A.scal + SC_T);
+    if (!(t < __ldcg(A.scal + SC_TEND))) return;  // run_until predicate (uniform per grid)
+    const double dtd = __ldcg(A.scal + SC_DT);
     const float dt = (float)dtd;
     const int npx = P.npx, npy = P.npy;
     const bool periodic = (P.wbc == 2);
     const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int x0 = bx * TX, y0 = by * TY;
     const long long pitch = A.pitch, plane = A.plane;
     const double eta0 = P.eta0;
 
@@ -146,7 +157,7 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
         V0 = A.bufA;
         Vout = FIRST ? A.bufB : A.bufA;
     } else {
-        par = (int)A.scal[SC_PAR];
+        par = (int)__ldcg(A.scal + SC_PAR);
         Vin = par ? A.bufB : A.bufA;
         V0 = Vin;
         Vout = par ? A.bufA : A.bufB;
@@ -159,8 +170,8 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
         int gy = wrap_clamp32(y0 + ly - 2, npy, periodic);
         long long g = (long long)gy * pitch + gx;
 #pragma unroll
-        for (int f = 0; f < 5; f++) sV[f * PS + idx] = Vin[f * plane + g];
-        sM[idx] = A.mask[g];
+        for (int f = 0; f < 5; f++) sV[f * PS + idx] = __ldg(Vin + f * plane + g);
+        sM[idx] = __ldg(A.mask + g);
     }
     const int tx = tid % TX, ty = tid / TX;
     const int gi = x0 + tx, gj = y0 + ty;
@@ -169,13 +180,13 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
     float v0[5];
     if (!FIRST) {
 #pragma unroll
-        for (int f = 0; f < 5; f++) v0[f] = V0[f * plane + gown];
+        for (int f = 0; f < 5; f++) v0[f] = __ldcg(V0 + f * plane + gown);
     }
     float ex_h = 0.f, ex_b = 0.f, ex_e = 0.f;  // running extrema, loaded early
     if (LAST && own) {
-        ex_h = A.hmax[gown];
-        ex_b = A.bmin[gown];
-        ex_e = A.eta_max[gown];
+        ex_h = __ldcg(A.hmax + gown);
+        ex_b = __ldcg(A.bmin + gown);
+        ex_e = __ldcg(A.eta_max + gown);
     }
     __syncthreads();
     const int cidx = (ty + 2) * LX + (tx + 2);
@@ -187,7 +198,7 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
         for (int f = 0; f < 5; f++) v0[f] = vc[f];
     }
 
-    // ---- phase 2: depth (FP64 island), velocity, concentration per cell
+    // ---- phase 2: depth, velocity, concentration per cell
     for (int idx = tid; idx < PS; idx += NT) {
         const float zz = sV[idx], HH = sV[PS + idx];
         const float hs = zz + (P.eta0f + HH);  // FP32 when clearly wet, FP64 near dryness
@@ -230,7 +241,7 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
         Face32 fm, fp;
         if (ORDER == 2) {
             float deta;
-            recon32(P, sV, c, c - step, c + step, fm, fp, deta);
+            recon32<PS>(P, sV, c, c - step, c + step, fm, fp, deta);
             if (didx >= 0) sDeta[didx] = deta;
         } else {
             fm.h = sV[5 * PS + c];
@@ -247,7 +258,7 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
     __syncthreads();
 
     // ---- phase 4: edges
-    const bool series_on = P.read_files && (t < A.tCC[A.timeCC - 2]);
+    const bool series_on = P.read_files && (t < __ldg(A.tCC + (A.timeCC - 2)));
     constexpr int NV = (TX + 1) * TY, NH = TX * (TY + 1);
     constexpr int FS = TY * TX;
     for (int item = tid; item < NV + NH; item += NT) {
@@ -361,10 +372,10 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
         float Dm[5], Dp[5];
         edge32(P, a, qna, qta, b, qnb, qtb, fixed, Dm, Dp);
         // back to x/y: x edges (nx = sgnn, ny = 0), y edges (nx = 0, ny = sgnn)
-        float m1 = vert ? sgnn * Dm[1] : -sgnn * Dm[2];
-        float m2 = vert ? sgnn * Dm[2] : sgnn * Dm[1];
-        float p1 = vert ? sgnn * Dp[1] : -sgnn * Dp[2];
-        float p2 = vert ? sgnn * Dp[2] : sgnn * Dp[1];
+        const float m1 = vert ? sgnn * Dm[1] : -sgnn * Dm[2];
+        const float m2 = vert ? sgnn * Dm[2] : sgnn * Dm[1];
+        const float p1 = vert ? sgnn * Dp[1] : -sgnn * Dp[2];
+        const float p2 = vert ? sgnn * Dp[2] : sgnn * Dp[1];
         if (outM) {
             outM[0] = Dm[0];
             outM[FS] = m1;
@@ -444,17 +455,17 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
             qy = h * uy;
             hc = h * c;
         }
-        Vout[gown] = z;
-        Vout[plane + gown] = H;
-        Vout[2 * plane + gown] = qx;
-        Vout[3 * plane + gown] = qy;
-        Vout[4 * plane + gown] = hc;
+        __stcg(Vout + gown, z);
+        __stcg(Vout + plane + gown, H);
+        __stcg(Vout + 2 * plane + gown, qx);
+        __stcg(Vout + 3 * plane + gown, qy);
+        __stcg(Vout + 4 * plane + gown, hc);
         if (LAST) {
             if (h > P.eps_h) {
-                A.hmax[gown] = fmaxf(ex_h, h);
-                A.eta_max[gown] = fmaxf(ex_e, (float)((double)z + eta0));
+                __stcg(A.hmax + gown, fmaxf(ex_h, h));
+                __stcg(A.eta_max + gown, fmaxf(ex_e, (float)((double)z + eta0)));
             }
-            A.bmin[gown] = fmaxf(ex_b, H);
+            __stcg(A.bmin + gown, fmaxf(ex_b, H));
             const float d = cfl_dt32(P, h, qx, qy);
             if (!isnan(d)) dtcell = d;
             mass = fmax(hd, 0.0);
@@ -483,18 +494,15 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
                 ms += sRed[kWarps + w];
                 sd += sRed[2 * kWarps + w];
             }
-            const unsigned nb = gridDim.x * gridDim.y;
-            const unsigned bI = blockIdx.y * gridDim.x + blockIdx.x;
-            A.partials[bI] = mm;
-            A.partials[nb + bI] = ms;
-            A.partials[2 * nb + bI] = sd;
+            __stcg(A.partials + blin, mm);
+            __stcg(A.partials + nb + blin, ms);
+            __stcg(A.partials + 2 * nb + blin, sd);
             __threadfence();
             sLast = (atomicAdd(A.ticket, 1u) == nb - 1);
         }
         __syncthreads();
         if (sLast) {
             __threadfence();
-            const unsigned nb = gridDim.x * gridDim.y;
             // every thread owns a fixed strided subset and the tree below has a
             // fixed shape, so the FP64 sums do not depend on CTA timing
             double mm = CUDART_INF, ms = 0.0, sd = 0.0;
@@ -537,6 +545,65 @@ __global__ void __launch_bounds__(NT, 2) stage32_kernel(Stage32Args A) {
         }
     }
 }
+
+// ---- single grid: one CTA per tile
+template <int TX, int TY, int MINB, int ORDER, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(TX *TY, MINB) stage32_kernel(Stage32Args A) {
+    extern __shared__ __align__(16) float smem32[];
+    stage32_tile<TX, TY, ORDER, FIRST, LAST>(A, A.phys, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x,
+                                             gridDim.x * gridDim.y, smem32);
+}
+
+// ---- ensemble: persistent CTAs walking the tile list of all members
+// (static stride or a dynamic work counter); each member keeps its own
+// time, dt (segmented min-reduction by the member's last CTA), extrema and
+// sums.  The member descriptor (buffers) is staged in shared memory per
+// tile; the physical parameters shared by all members come in as a kernel
+// parameter (constant-bank operands in the flux arithmetic) and only the
+// grid fields (size, spacing, still-water level, boundary switches) are
+// taken from the member.
+template <int TX, int TY, int MINB, int ORDER, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(TX *TY, MINB) ens32_kernel(EnsArgs E, Phys32 common) {
+    extern __shared__ __align__(16) float smem32[];
+    __shared__ Stage32Args sG;
+    __shared__ unsigned sTile;
+    unsigned tile = blockIdx.x;
+    if (E.dynamic) {
+        if (threadIdx.x == 0) sTile = atomicAdd(E.work, 1u);
+        __syncthreads();
+        tile = sTile;
+    }
+    while (tile < E.ntiles) {
+        const int m = E.tile_member[tile];
+        if (threadIdx.x == 0) sG = E.members[m].g;
+        __syncthreads();
+        const unsigned lt = tile - E.members[m].tile0;
+        const int ntx = E.members[m].ntx;
+        Phys32 P = common;
+        P.eta0 = sG.phys.eta0;
+        P.eta0f = sG.phys.eta0f;
+        P.dx = sG.phys.dx;
+        P.dy = sG.phys.dy;
+        P.inv_dx = sG.phys.inv_dx;
+        P.inv_dy = sG.phys.inv_dy;
+        P.npx = sG.phys.npx;
+        P.npy = sG.phys.npy;
+        P.wbc = sG.phys.wbc;
+        P.read_files = sG.phys.read_files;
+        stage32_tile<TX, TY, ORDER, FIRST, LAST>(sG, P, lt % ntx, lt / ntx, lt, E.members[m].ntiles, smem32);
+        __syncthreads();
+        if (E.dynamic) {
+            if (threadIdx.x == 0) sTile = atomicAdd(E.work, 1u);
+            __syncthreads();
+            tile = sTile;
+            __syncthreads();
+        } else {
+            tile += gridDim.x;
+        }
+    }
+}
+
+__global__ void reset_work_kernel(unsigned *w) { *w = 0u; }
 
 // FP64 host planes (device copy) -> FP32 state; and back.
 __global__ void to32_kernel(const double *__restrict__ V64, long long pitch, long long plane, int npx, int npy,
@@ -628,25 +695,126 @@ __global__ void __launch_bounds__(256) dt32_kernel(const float *__restrict__ V, 
 }
 
 // ------------------------------------------------------------------ host side
-cudaError_t stage32_prepare() {
-    const int sm = (int)stage32_smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(stage32_kernel<2, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(stage32_kernel<2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(stage32_kernel<1, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    return e;
+namespace {
+
+struct Variant32 {
+    int tx, ty, minb;
+    size_t smem;
+    void (*k[3])(Stage32Args);
+    void (*e[3])(EnsArgs, Phys32);
+};
+
+template <int TX, int TY, int MINB>
+Variant32 make_variant32() {
+    Variant32 v;
+    v.tx = TX;
+    v.ty = TY;
+    v.minb = MINB;
+    v.smem = T32<TX, TY>::smem();
+    v.k[0] = stage32_kernel<TX, TY, MINB, 2, true, false>;
+    v.k[1] = stage32_kernel<TX, TY, MINB, 2, false, true>;
+    v.k[2] = stage32_kernel<TX, TY, MINB, 1, true, true>;
+    v.e[0] = ens32_kernel<TX, TY, MINB, 2, true, false>;
+    v.e[1] = ens32_kernel<TX, TY, MINB, 2, false, true>;
+    v.e[2] = ens32_kernel<TX, TY, MINB, 1, true, true>;
+    return v;
 }
 
-dim3 stage32_grid(int npx, int npy) { return dim3((npx + TX - 1) / TX, (npy + TY - 1) / TY); }
+// tile W x H / minimum resident CTAs per SM (register budget)
+const Variant32 *variants32(int *n) {
+    static Variant32 v[7] = {make_variant32<32, 8, 2>(),  make_variant32<16, 16, 2>(), make_variant32<32, 16, 1>(),
+                             make_variant32<64, 4, 2>(),  make_variant32<32, 8, 3>(),  make_variant32<16, 16, 3>(),
+                             make_variant32<32, 8, 4>()};
+    if (n) *n = 7;
+    return v;
+}
+
+// single-grid variant: TSU_TILE32 = index into variants32; default 32x8
+// with 4 resident CTAs per SM (measured fastest: 32 warps per SM hide the
+// fixed-latency dependencies of the flux arithmetic; 16 warps did not)
+constexpr int kSingleDefault = 6;
+int single_variant() {
+    static int k = [] {
+        int n;
+        variants32(&n);
+        const char *e = std::getenv("TSU_TILE32");
+        const int i = e ? std::atoi(e) : kSingleDefault;
+        return (i >= 0 && i < n) ? i : kSingleDefault;
+    }();
+    return k;
+}
+
+int which(int order, int stage) { return (order == 2) ? (stage == 0 ? 0 : 1) : 2; }
+
+}  // namespace
+
+bool phys32_shared(const Phys32 &a, const Phys32 &b) {
+    Phys32 x = a, y = b;
+    for (Phys32 *q : {&x, &y}) {  // clear the per-member grid fields
+        q->eta0 = 0.0;
+        q->eta0f = q->dx = q->dy = q->inv_dx = q->inv_dy = 0.f;
+        q->npx = q->npy = q->wbc = q->read_files = 0;
+    }
+    return x.FR == y.FR && x.eps_h == y.eps_h && x.Opar == y.Opar && x.OC == y.OC && x.Q == y.Q && x.HQB == y.HQB &&
+           x.porosity == y.porosity && x.CFL == y.CFL && x.vs == y.vs && x.A_er == y.A_er && x.sqrt_FR == y.sqrt_FR &&
+           x.VP == y.VP && x.K_dep == y.K_dep && x.sqrt_OC == y.sqrt_OC && x.DS5 == y.DS5 && x.inv_vs == y.inv_vs &&
+           x.order == y.order && x.bedload == y.bedload && x.suspension == y.suspension &&
+           x.bedload_law == y.bedload_law && x.grass_ag == y.grass_ag;
+}
+
+int stage32_num_tiles() {
+    int n;
+    variants32(&n);
+    return n;
+}
+
+void stage32_tile_shape(int variant, int *tx, int *ty, int *minb) {
+    const Variant32 &v = variants32(nullptr)[variant];
+    *tx = v.tx;
+    *ty = v.ty;
+    *minb = v.minb;
+}
+
+size_t stage32_smem_bytes() { return variants32(nullptr)[single_variant()].smem; }
+
+cudaError_t stage32_prepare() {
+    int n;
+    const Variant32 *v = variants32(&n);
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < 3; i++) {
+            cudaError_t e = cudaFuncSetAttribute(v[j].k[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v[j].smem);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(v[j].e[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v[j].smem);
+            if (e != cudaSuccess) return e;
+        }
+    return cudaSuccess;
+}
+
+dim3 stage32_grid(int npx, int npy) {
+    const Variant32 &v = variants32(nullptr)[single_variant()];
+    return dim3((npx + v.tx - 1) / v.tx, (npy + v.ty - 1) / v.ty);
+}
 
 cudaError_t stage32_launch(int order, int stage, const Stage32Args &a, cudaStream_t st) {
+    const Variant32 &v = variants32(nullptr)[single_variant()];
     dim3 g = stage32_grid(a.phys.npx, a.phys.npy);
-    size_t sm = stage32_smem_bytes();
-    if (order == 2 && stage == 0) stage32_kernel<2, true, false><<<g, NT, sm, st>>>(a);
-    else if (order == 2) stage32_kernel<2, false, true><<<g, NT, sm, st>>>(a);
-    else stage32_kernel<1, true, true><<<g, NT, sm, st>>>(a);
+    v.k[which(order, stage)]<<<g, v.tx * v.ty, v.smem, st>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t ens32_launch(int variant, int order, int stage, const EnsArgs &e, const Phys32 &common, int ctas,
+                         cudaStream_t st) {
+    const Variant32 &v = variants32(nullptr)[variant];
+    if (e.dynamic) reset_work_kernel<<<1, 1, 0, st>>>(e.work);
+    v.e[which(order, stage)]<<<ctas, v.tx * v.ty, v.smem, st>>>(e, common);
+    return cudaGetLastError();
+}
+
+int ens32_max_ctas_per_sm(int variant) {
+    const Variant32 &v = variants32(nullptr)[variant];
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, v.e[1], v.tx * v.ty, v.smem);
+    return n;
 }
 
 cudaError_t to32_launch(const double *V64, long long pitch, long long plane, int npx, int npy, double eta0, float *V32,

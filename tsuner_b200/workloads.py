@@ -199,3 +199,29 @@ def humps_shelf(npx=8192, npy=8192, dx=5.0, steps=2000, seed=3, slr=0.0, nhumps=
     p = make_params(npx, npy, dx, dx)
     sw = make_switches(order=2, wbc=1, read_files=0, eta0=slr)
     return Workload("humps%dx%d" % (npx, npy), p, sw, V, mask, slr=slr, steps=steps)
+
+
+def ensemble(nmembers=256, lo=256, hi=2048, seed=4, dx=5.0, slr=0.5, t_series=400.0):
+    """Config 4: `nmembers` members on square grids whose sides are drawn
+    log-uniform in [lo, hi] (seed 4), each with its own seeded shelf
+    bathymetry, harbour mask and west-boundary N-wave (amplitude 1-5 m,
+    period 300-1200 s); FP32 precision form."""
+    rng = np.random.default_rng(seed)
+    sides = np.exp(rng.uniform(np.log(lo), np.log(hi), nmembers)).astype(int)
+    amps = rng.uniform(1.0, 5.0, nmembers)
+    periods = rng.uniform(300.0, 1200.0, nmembers)
+    seeds = rng.integers(0, 2 ** 31, nmembers)
+    out = []
+    for k in range(nmembers):
+        n = int(sides[k])
+        mr = np.random.default_rng(int(seeds[k]))
+        H = shelf_bathymetry(n, n, dx, mr, slr)
+        mask = harbour_mask(n, n, mr)
+        V = np.zeros((5, n, n))
+        V[0] = np.maximum(slr + H, 0.0)
+        V[3] = H
+        CC, tCC = boundary_series(H, slr, t_series, amp=float(amps[k]), period=float(periods[k]))
+        p = make_params(n, n, dx, dx)
+        sw = make_switches(order=2, wbc=1, read_files=1, precision=1, eta0=slr)
+        out.append(Workload("member%d_%d" % (k, n), p, sw, V, mask, CC, tCC, slr=slr))
+    return out
