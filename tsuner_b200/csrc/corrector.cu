@@ -65,10 +65,13 @@ constexpr int KROWS = 9 * C;                // 288
 constexpr unsigned long long kWaitNs = 500000000ull;  // 0.5 s per wait
 
 constexpr int kFwdSmem = 1024 + kWBytes + 2 * kPatch + 64;
-// wgrad: patch + dZ tile + A (8 K steps x 3 M blocks x 4 KB)
+// wgrad: patch + dZ tile + A for half of the 8 K steps (4 x 3 M blocks x 4 KB);
+// ~67 KB, so three CTAs fit on an SM
 constexpr int kZPlane = 128 * 16;
 constexpr int kABlock = 4096;
-constexpr int kWgSmem = 1024 + kPatch + 4 * kZPlane + 8 * 3 * kABlock + 64;
+constexpr int kWgHalf = 4;
+constexpr int kWgSmem = 1024 + kPatch + 4 * kZPlane + kWgHalf * 3 * kABlock + 64;
+constexpr int kWgCtasPerSm = 3;
 
 __device__ int g_corr_err;  // set by a kernel whose wait expired
 
@@ -337,7 +340,7 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a) {
 }
 
 // Weight (and bias) gradient, accumulated into dW[cout][288] and db[32].
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, kWgCtasPerSm)
     conv3x3_wgrad_kernel(const bf16 *__restrict__ X, const bf16 *__restrict__ dZ, int nimg, int H, int W,
                          float *__restrict__ dW, float *__restrict__ db) {
     extern __shared__ unsigned char sm_raw[];
@@ -345,14 +348,14 @@ __global__ void __launch_bounds__(128, 1)
     unsigned char *sP = sm;
     unsigned char *sZ = sm + kPatch;
     unsigned char *sA = sZ + 4 * kZPlane;
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(sA + 24 * kABlock);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sA + kWgHalf * 3 * kABlock);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TileGeom G = tile_geom(nimg, H, W);
 
     // rows 288..383 of A: zero, except row 288 = 1 (bias gradient); these
     // core matrices (M groups 36..47 = block 2 groups 4..15) are never rewritten
-    for (int c = tid; c < 8 * 12 * 2 * 8; c += 128) {  // (s, group, kgroup, 16-byte row)
+    for (int c = tid; c < kWgHalf * 12 * 2 * 8; c += 128) {  // (s, group, kgroup, 16-byte row)
         const int r = c & 7, kg = (c >> 3) & 1, g = 4 + ((c >> 4) % 12), s = c / 192;
         uint4 v = make_uint4(0, 0, 0, 0);
         if (g == 4) v.x = 0x3F80u;  // bf16 1.0 in element 0: row 288 of this pixel
@@ -371,7 +374,7 @@ __global__ void __launch_bounds__(128, 1)
     const uint32_t a_u32 = smem_u32(sA), z_u32 = smem_u32(sZ);
 
     bool failed = false;
-    int i = 0;
+    int i = 0, nwait = 0;
     for (int t = blockIdx.x; t < G.total; t += gridDim.x, i++) {
         const int img = t / G.per_img, r = t - img * G.per_img;
         const int tyi = r / G.ntx, txi = r - tyi * G.ntx;
@@ -388,41 +391,49 @@ __global__ void __launch_bounds__(128, 1)
         cp_async_commit();
         cp_async_wait_all();
         __syncthreads();
-        // A core matrices (s, G = tap*4 + quarter, kgroup): 8 pixels of tile
-        // row 2s + kg shifted by the tap, 8 channels each
-        for (int c = tid; c < 8 * 36 * 2; c += 128) {
-            const int s = c / 72, rem = c - s * 72, Gm = rem >> 1, kg = rem & 1;
-            const int tap = Gm >> 2, q = Gm & 3, dy = tap / 3, dx = tap - dy * 3;
-            const int py = 2 * s + kg;
-            const uint4 *src = reinterpret_cast<const uint4 *>(sP + q * kPlane + ((py + dy) * PW + dx) * 16);
-            uint4 *dst = reinterpret_cast<uint4 *>(sA + (s * 3 + (Gm >> 4)) * kABlock + (Gm & 15) * 256 + kg * 128);
-#pragma unroll
-            for (int k = 0; k < 8; k++) dst[k] = src[k];
-        }
-        fence_async_smem();
-        fence_before();
-        __syncthreads();
-        fence_after();
-        if (tid == 0) {
-#pragma unroll 1
-            for (int s = 0; s < 8; s++) {
-                const uint64_t dbd = sdesc(z_u32 + s * 256, 128, kZPlane);
-#pragma unroll
-                for (int b = 0; b < 3; b++) {
-                    const uint64_t da = sdesc(a_u32 + (s * 3 + b) * kABlock, 128, 256);
-                    mma_bf16(tmem + (uint32_t)(b * 32), da, dbd, id, (i > 0 || s > 0) ? 1u : 0u);
-                }
+        // two rounds of 4 K steps (tile rows 0-7, then 8-15)
+        for (int hh = 0; hh < 2 && !failed; hh++) {
+            // A core matrices (s, G = tap*4 + quarter, kgroup): 8 pixels of
+            // tile row 2s + kg shifted by the tap, 8 channels each; 8 lanes
+            // copy one 128-byte core matrix (no bank conflicts)
+            for (int c = tid; c < kWgHalf * 36 * 2 * 8; c += 128) {
+                const int k = c & 7, blk = c >> 3;
+                const int sl = blk / 72, rem = blk - sl * 72, Gm = rem >> 1, kg = rem & 1;
+                const int tap = Gm >> 2, q = Gm & 3, dy = tap / 3, dx = tap - dy * 3;
+                const int py = 2 * (kWgHalf * hh + sl) + kg;
+                const uint4 *src = reinterpret_cast<const uint4 *>(sP + q * kPlane + ((py + dy) * PW + dx) * 16);
+                uint4 *dst =
+                    reinterpret_cast<uint4 *>(sA + (sl * 3 + (Gm >> 4)) * kABlock + (Gm & 15) * 256 + kg * 128);
+                dst[k] = src[k];
             }
-            mma_commit(mbar);
+            fence_async_smem();
+            fence_before();
+            __syncthreads();
+            fence_after();
+            if (tid == 0) {
+#pragma unroll 1
+                for (int sl = 0; sl < kWgHalf; sl++) {
+                    const int s = kWgHalf * hh + sl;
+                    const uint64_t dbd = sdesc(z_u32 + s * 256, 128, kZPlane);
+#pragma unroll
+                    for (int b = 0; b < 3; b++) {
+                        const uint64_t da = sdesc(a_u32 + (sl * 3 + b) * kABlock, 128, 256);
+                        mma_bf16(tmem + (uint32_t)(b * 32), da, dbd, id, (i > 0 || s > 0) ? 1u : 0u);
+                    }
+                }
+                mma_commit(mbar);
+            }
+            // the A buffer is rewritten by the next round: wait for these MMAs
+            const bool ok = mbar_wait(mbar, nwait & 1);
+            nwait++;
+            if (__syncthreads_or(!ok)) {
+                failed = true;
+                if (tid == 0) atomicExch(&g_corr_err, 1);
+                mbar_wait(mbar, (nwait - 1) & 1);
+            }
+            fence_after();
         }
-        const bool ok = mbar_wait(mbar, i & 1);
-        if (__syncthreads_or(!ok)) {
-            failed = true;
-            if (tid == 0) atomicExch(&g_corr_err, 1);
-            mbar_wait(mbar, i & 1);
-            break;
-        }
-        fence_after();
+        if (failed) break;
     }
     if (!failed && i > 0) {
 #pragma unroll 1
@@ -600,7 +611,7 @@ cudaError_t wgrad_launch(const bf16 *X, const bf16 *dZ, int nimg, int H, int W, 
     cudaError_t e = prepare();
     if (e != cudaSuccess) return e;
     const TileGeom G = tile_geom(nimg, H, W);
-    const int ctas = std::min(G.total, num_sms());
+    const int ctas = std::min(G.total, kWgCtasPerSm * num_sms());
     conv3x3_wgrad_kernel<<<ctas, 128, kWgSmem, st>>>(X, dZ, nimg, H, W, dW, db);
     return cudaGetLastError();
 }
