@@ -81,3 +81,36 @@ def test_autotune_restores_state_and_picks_a_config(reference_runs):
         assert np.array_equal(s.state(), ref[k][0])
         assert s.time()[2] == STEPS
     e.close()
+
+
+def test_run_until_stops_each_member_at_its_end_time(reference_runs):
+    """tsu_ens_run_until: every member reaches t_end with its own step count
+    and then skips its tiles; each member's state equals the same member run
+    alone with tsu_run_until."""
+    ws, _ = reference_runs
+    t_end = 6.0
+    alone = []
+    for w in ws:
+        s = T.Solver(w.p, w.sw)
+        s.set_state(w.V)
+        s.set_mask(w.mask)
+        if w.sw.read_files:
+            s.set_boundary_series(w.CC, w.tCC)
+        s.reset()
+        s.run_until(t_end)
+        alone.append((s.state(), s.time()))
+        s.close()
+    e = make_ens(ws)
+    e.run_until(t_end)
+    e.sync()
+    for k, s in enumerate(e.members):
+        t, dt, n = s.time()
+        assert t >= t_end
+        assert (t, dt, n) == alone[k][1]
+        assert np.array_equal(s.state(), alone[k][0])
+    steps = {s.time()[2] for s in e.members}
+    assert len(steps) > 1  # members needed different numbers of steps
+    e.step(1)  # run_until restores the open end time
+    e.sync()
+    assert all(s.time()[2] == alone[k][1][2] + 1 for k, s in enumerate(e.members))
+    e.close()

@@ -76,26 +76,27 @@ __device__ __forceinline__ float limiter32(float a, float b) {
     return (p > 0.f) ? __fdividef(2.f * p, a + b) : 0.f;
 }
 
+// A reconstructed face after the state filter: depth, surface deviation,
+// (clamped) velocity, bed, concentration.  The edge flux works on velocity
+// and concentration, so they are kept instead of discharge and load.
 struct Face32 {
-    float h, z, qx, qy, H, hc;
+    float h, z, u, v, H, c;
 };
 
-// state_filter (GPU/SedFlux.cuh:103-117) on a face; a clipped face becomes a
-// dry face (z from its bed).
-__device__ __forceinline__ void filter32(Face32 &f, double eta0) {
+// state_filter (GPU/SedFlux.cuh:103-117) of a face with discharges qx, qy and
+// concentration cf (load / depth); a clipped face becomes a dry face (z from
+// its bed).
+__device__ __forceinline__ void filter32(Face32 &f, float qx, float qy, float cf, double eta0) {
     if (!(f.h > 0.f)) {
         f.h = 0.f;
-        f.qx = f.qy = 0.f;
-        f.hc = 0.f;
+        f.u = f.v = 0.f;
+        f.c = 0.f;
         f.z = dry_z(f.H, eta0);
         return;
     }
-    float ux, uy, m;
-    velocity32(f.h, f.qx, f.qy, ux, uy, m);
-    float c = fmaxf(f.hc * __frcp_rn(f.h), 0.f);
-    f.qx = f.h * ux;
-    f.qy = f.h * uy;
-    f.hc = f.h * c;
+    float m;
+    velocity32(f.h, qx, qy, f.u, f.v, m);
+    f.c = fmaxf(cf, 0.f);
 }
 
 // bedload (GPU/SedFlux.cuh:150-168) / Grass law.
@@ -108,16 +109,13 @@ __device__ __forceinline__ float bedload32(const Phys32 &P, float h, float ux, f
 }
 
 // One edge (RiemannSolver_Vols, GPU/VolumeSolver.cu:19-126) in the rotated
-// frame.  a leaves along the normal, b is entered.  Normal-frame momenta:
-// qn = n.q, qt = n x q.  Outputs Dm (into a), Dp (into b) in the normal frame
-// (components h, qn, qt, H, hc).
-__device__ __forceinline__ void edge32(const Phys32 &P, const Face32 &a, float qna, float qta, const Face32 &b,
-                                       float qnb, float qtb, int fixed, float Dm[5], float Dp[5]) {
-    float u0, v0, m0, u1, v1, m1;
-    velocity32(a.h, qna, qta, u0, v0, m0);
-    velocity32(b.h, qnb, qtb, u1, v1, m1);
-    float c0 = (a.h > 0.f) ? a.hc * __frcp_rn(a.h) : 0.f;
-    float c1 = (b.h > 0.f) ? b.hc * __frcp_rn(b.h) : 0.f;
+// frame.  a leaves along the normal, b is entered.  Normal-frame velocities:
+// un = n.u, ut = n x u (the faces' filtered velocities, so the division of
+// the reference's u_calculator is not repeated here).  Outputs Dm (into a),
+// Dp (into b) in the normal frame (components h, qn, qt, H, hc).
+__device__ __forceinline__ void edge32(const Phys32 &P, const Face32 &a, float u0, float v0, const Face32 &b,
+                                       float u1, float v1, int fixed, float Dm[5], float Dp[5]) {
+    const float c0 = a.c, c1 = b.c;
     // hydrostatic reconstruction h* = max(eta + min(H_a, H_b), 0), eta = z + eta0:
     // on an edge that is wet by a clear margin on both sides the depths are
     // formed in FP32 and their difference is the exact difference of the
@@ -146,8 +144,8 @@ __device__ __forceinline__ void edge32(const Phys32 &P, const Face32 &a, float q
     F1[2] = F1[0] * v1;
     F1[4] = h1 * c1 * u1;
     if (fixed && P.bedload) {
-        F0[3] = bedload32(P, h0, u0, m0);
-        F1[3] = bedload32(P, h1, u1, m1);
+        F0[3] = bedload32(P, h0, u0, sqrtf(u0 * u0 + v0 * v0));
+        F1[3] = bedload32(P, h1, u1, sqrtf(u1 * u1 + v1 * v1));
     } else {
         F0[3] = F1[3] = 0.f;
     }
@@ -200,6 +198,13 @@ __device__ __forceinline__ void edge32(const Phys32 &P, const Face32 &a, float q
 __device__ __forceinline__ float cfl_dt32(const Phys32 &P, float h, float qx, float qy) {
     float ux, uy, m;
     velocity32(h, qx, qy, ux, uy, m);
+    float cg = sqrtf(kGf * h);
+    float lx = fabsf(ux) + cg, ly = fabsf(uy) + cg;
+    return P.CFL * 0.5f * fminf(P.dx / lx, P.dy / ly);
+}
+
+// The same from the velocity of the filtered state (the update has it).
+__device__ __forceinline__ float cfl_dt32v(const Phys32 &P, float h, float ux, float uy) {
     float cg = sqrtf(kGf * h);
     float lx = fabsf(ux) + cg, ly = fabsf(uy) + cg;
     return P.CFL * 0.5f * fminf(P.dx / lx, P.dy / ly);

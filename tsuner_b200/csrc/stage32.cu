@@ -44,19 +44,19 @@ __device__ __forceinline__ int wrap_clamp32(int g, int n, bool periodic) {
 __device__ __forceinline__ void put_face(float *base, int stride, const Face32 &f) {
     base[0] = f.h;
     base[stride] = f.z;
-    base[2 * stride] = f.qx;
-    base[3 * stride] = f.qy;
+    base[2 * stride] = f.u;
+    base[3 * stride] = f.v;
     base[4 * stride] = f.H;
-    base[5 * stride] = f.hc;
+    base[5 * stride] = f.c;
 }
 __device__ __forceinline__ Face32 get_face(const float *base, int stride) {
     Face32 f;
     f.h = base[0];
     f.z = base[stride];
-    f.qx = base[2 * stride];
-    f.qy = base[3 * stride];
+    f.u = base[2 * stride];
+    f.v = base[3 * stride];
     f.H = base[4 * stride];
-    f.hc = base[5 * stride];
+    f.c = base[5 * stride];
     return f;
 }
 
@@ -102,18 +102,15 @@ __device__ __forceinline__ void recon32(const Phys32 &P, const float *s, int c, 
     const float uix = s[6 * PS + c], uiy = s[7 * PS + c];
     float du = limiter32(uix - s[6 * PS + l], s[6 * PS + r] - uix);
     float dq = hi * du + uix * dh;
-    fm.qx = s[2 * PS + c] - 0.5f * dq;
-    fp.qx = s[2 * PS + c] + 0.5f * dq;
+    const float qxm = s[2 * PS + c] - 0.5f * dq, qxp = s[2 * PS + c] + 0.5f * dq;
     du = limiter32(uiy - s[7 * PS + l], s[7 * PS + r] - uiy);
     dq = hi * du + uiy * dh;
-    fm.qy = s[3 * PS + c] - 0.5f * dq;
-    fp.qy = s[3 * PS + c] + 0.5f * dq;
+    const float qym = s[3 * PS + c] - 0.5f * dq, qyp = s[3 * PS + c] + 0.5f * dq;
     const float ci = s[8 * PS + c];
     du = limiter32(ci - s[8 * PS + l], s[8 * PS + r] - ci);
-    fm.hc = (ci - 0.5f * du) * fm.h;
-    fp.hc = (ci + 0.5f * du) * fp.h;
-    filter32(fm, P.eta0);
-    filter32(fp, P.eta0);
+    // face load (ci -+ dc/2) h_face: its concentration is ci -+ dc/2
+    filter32(fm, qxm, qym, ci - 0.5f * du, P.eta0);
+    filter32(fp, qxp, qyp, ci + 0.5f * du, P.eta0);
 }
 
 // One RK stage on tile (bx, by) of grid A.  blin / nb: linear index of the
@@ -163,12 +160,19 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         Vout = par ? A.bufA : A.bufB;
     }
 
+    // tile and halo inside the grid, not periodic: no clamping, and every
+    // edge of the tile is an interior edge
+    const bool inner = !periodic && x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= npx && y0 + TY + 2 <= npy;
+
     // ---- phase 1: load z, H, qx, qy, hc (+mask) with a 2-cell halo
     for (int idx = tid; idx < PS; idx += NT) {
-        int ly = idx / LX, lx = idx - ly * LX;
-        int gx = wrap_clamp32(x0 + lx - 2, npx, periodic);
-        int gy = wrap_clamp32(y0 + ly - 2, npy, periodic);
-        long long g = (long long)gy * pitch + gx;
+        const int ly = idx / LX, lx = idx - ly * LX;
+        int gx = x0 + lx - 2, gy = y0 + ly - 2;
+        if (!inner) {
+            gx = wrap_clamp32(gx, npx, periodic);
+            gy = wrap_clamp32(gy, npy, periodic);
+        }
+        const long long g = (long long)gy * pitch + gx;
 #pragma unroll
         for (int f = 0; f < 5; f++) sV[f * PS + idx] = __ldg(Vin + f * plane + g);
         sM[idx] = __ldg(A.mask + g);
@@ -247,9 +251,9 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             fm.h = sV[5 * PS + c];
             fm.z = sV[c];
             fm.H = sV[PS + c];
-            fm.qx = sV[2 * PS + c];
-            fm.qy = sV[3 * PS + c];
-            fm.hc = sV[4 * PS + c];
+            fm.u = sV[6 * PS + c];
+            fm.v = sV[7 * PS + c];
+            fm.c = sV[8 * PS + c];
             fp = fm;
         }
         put_face(dst, fstride, fm);
@@ -257,24 +261,42 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     }
     __syncthreads();
 
-    // ---- phase 4: edges
-    const bool series_on = P.read_files && (t < __ldg(A.tCC + (A.timeCC - 2)));
+    // ---- phase 4: edges.  One call site of the edge flux serves every kind
+    // of edge, so the arithmetic (and its contraction into FMAs) of an edge
+    // does not depend on which tile, tile shape or schedule computes it.
     constexpr int NV = (TX + 1) * TY, NH = TX * (TY + 1);
     constexpr int FS = TY * TX;
+    const bool series_on = !inner && P.read_files && (t < __ldg(A.tCC + (A.timeCC - 2)));
     for (int item = tid; item < NV + NH; item += NT) {
         Face32 a, b;
-        int sgnn, fixed, seg = 0;
-        bool bnd = false, seam = false, vert;
+        int sgnn = 1, fixed, seg = 0;
+        bool bnd = false, seam = false;
+        const bool vert = item < NV;
         float *outM = nullptr, *outP = nullptr;
-        if (item < NV) {
-            vert = true;
+        if (inner) {  // interior edges only (uniform per tile): no bounds or boundary cases
+            if (vert) {
+                const int r = item / (TX + 1), e = item - r * (TX + 1);
+                a = get_face(sFx + (6 * TY + r) * FXW + e, TY * FXW);
+                b = get_face(sFx + r * FXW + (e + 1), TY * FXW);
+                fixed = (int)sM[(r + 2) * LX + e + 1] * (int)sM[(r + 2) * LX + e + 2];
+                if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
+                if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
+            } else {
+                const int it = item - NV;
+                const int e = it / TX, c = it - e * TX;
+                a = get_face(sFy + (6 * FYH + e) * TX + c, FYH * TX);
+                b = get_face(sFy + (e + 1) * TX + c, FYH * TX);
+                fixed = (int)sM[(e + 1) * LX + c + 2] * (int)sM[(e + 2) * LX + c + 2];
+                if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
+                if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
+            }
+        } else if (vert) {
             const int r = item / (TX + 1), e = item - r * (TX + 1);
             const int ex = x0 + e, ey = y0 + r;
             if (ey >= npy || ex > npx) continue;
             const int ly = r + 2;
             const float *Rf = sFx + (6 * TY + r) * FXW + e;
             const float *Lf = sFx + r * FXW + (e + 1);
-            sgnn = 1;
             if (periodic && (ex == 0 || ex == npx)) {
                 a = get_face(Rf, TY * FXW);
                 b = get_face(Lf, TY * FXW);
@@ -304,14 +326,12 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
                 if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             }
         } else {
-            vert = false;
             const int it = item - NV;
             const int e = it / TX, c = it - e * TX;
             const int ex = x0 + c, ey = y0 + e;
             if (ex >= npx || ey > npy) continue;
             const float *Uf = sFy + (6 * FYH + e) * TX + c;
             const float *Df = sFy + (e + 1) * TX + c;
-            sgnn = 1;
             if (periodic && (ey == 0 || ey == npy)) {
                 a = get_face(Uf, FYH * TX);
                 b = get_face(Df, FYH * TX);
@@ -344,8 +364,8 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         if (bnd) {
             b = a;
             if (P.wbc == 1) {
-                if (vert) b.qx = -a.qx;
-                else b.qy = -a.qy;
+                if (vert) b.u = -a.u;
+                else b.v = -a.v;
             }
         }
         if ((bnd || seam) && P.read_files) {
@@ -355,22 +375,22 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
                 b.H = (float)g.H;
                 b.h = (float)fmax(g.h, 0.0);
                 b.z = (g.h > 0.0) ? (float)(g.h - g.H - eta0) : dry_z(b.H, eta0);
-                b.qx = (float)g.qx;
-                b.qy = (float)g.qy;
-                b.hc = 0.f;
+                float m;
+                velocity32(b.h, (float)g.qx, (float)g.qy, b.u, b.v, m);
+                b.c = 0.f;
             } else if (vert) {
-                b.qx = -a.qx;
+                b.u = -a.u;
             } else {
-                b.qy = -a.qy;
+                b.v = -a.v;
             }
         }
         // rotate to the edge normal: x edges n = (sgnn, 0), y edges n = (0, sgnn)
-        const float qna = vert ? sgnn * a.qx : sgnn * a.qy;
-        const float qta = vert ? sgnn * a.qy : -sgnn * a.qx;
-        const float qnb = vert ? sgnn * b.qx : sgnn * b.qy;
-        const float qtb = vert ? sgnn * b.qy : -sgnn * b.qx;
+        const float una = vert ? sgnn * a.u : sgnn * a.v;
+        const float uta = vert ? sgnn * a.v : -sgnn * a.u;
+        const float unb = vert ? sgnn * b.u : sgnn * b.v;
+        const float utb = vert ? sgnn * b.v : -sgnn * b.u;
         float Dm[5], Dp[5];
-        edge32(P, a, qna, qta, b, qnb, qtb, fixed, Dm, Dp);
+        edge32(P, a, una, uta, b, unb, utb, fixed, Dm, Dp);
         // back to x/y: x edges (nx = sgnn, ny = 0), y edges (nx = 0, ny = sgnn)
         const float m1 = vert ? sgnn * Dm[1] : -sgnn * Dm[2];
         const float m2 = vert ? sgnn * Dm[2] : sgnn * Dm[1];
@@ -402,8 +422,9 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             qx -= dt * P.inv_dx * kGf * hcell * sDeta[ty * TX + tx];
             qy -= dt * P.inv_dy * kGf * hcell * sDeta[TY * TX + ty * TX + tx];
         }
-        {  // friction + erosion/deposition from U^n
-            const float h0 = (float)depth64(v0[0], v0[1], eta0);
+        {  // friction + erosion/deposition from U^n (in the first stage U^n is
+           // this stage's input, whose depth phase 2 already formed)
+            const float h0 = FIRST ? hcell : (float)depth64(v0[0], v0[1], eta0);
             float ux, uy, modu;
             velocity32(h0, v0[2], v0[3], ux, uy, modu);
             const float cf = (h0 > 0.f) ? dt * P.FR * modu * __frcp_rn(h0) : 0.f;
@@ -441,18 +462,18 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             hc = 0.5f * (v0[4] + hc);
         }
         const double hd = (double)z + eta0 + (double)H;
-        float h;
+        float h, uxf = 0.f, uyf = 0.f;
         if (!(hd > 0.0)) {
             h = 0.f;
             z = dry_z(H, eta0);
             qx = qy = hc = 0.f;
         } else {
             h = (float)hd;
-            float ux, uy, m;
-            velocity32(h, qx, qy, ux, uy, m);
+            float m;
+            velocity32(h, qx, qy, uxf, uyf, m);
             const float c = fmaxf(hc * __frcp_rn(h), 0.f);
-            qx = h * ux;
-            qy = h * uy;
+            qx = h * uxf;
+            qy = h * uyf;
             hc = h * c;
         }
         __stcg(Vout + gown, z);
@@ -466,7 +487,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
                 __stcg(A.eta_max + gown, fmaxf(ex_e, (float)((double)z + eta0)));
             }
             __stcg(A.bmin + gown, fmaxf(ex_b, H));
-            const float d = cfl_dt32(P, h, qx, qy);
+            const float d = cfl_dt32v(P, h, uxf, uyf);
             if (!isnan(d)) dtcell = d;
             mass = fmax(hd, 0.0);
             sed = (double)H + (double)hc;
@@ -474,31 +495,38 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     }
 
     if (LAST) {
-        double m = (double)dtcell;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
-            mass += __shfl_xor_sync(0xffffffffu, mass, o);
-            sed += __shfl_xor_sync(0xffffffffu, sed, o);
-        }
-        if ((tid & 31) == 0) {
-            sRed[tid >> 5] = m;
-            sRed[kWarps + (tid >> 5)] = mass;
-            sRed[2 * kWarps + (tid >> 5)] = sed;
-        }
+        // dt: the minimum of non-negative floats (or +inf) is the minimum of
+        // their bit patterns, one warp reduction instruction
+        const unsigned mb = __reduce_min_sync(0xffffffffu, __float_as_uint(dtcell));
+        // FP64 water / sediment sums: per-thread values through shared memory
+        // (the face buffers are no longer needed), summed by warp 0 in a
+        // fixed order (strided per lane, then a fixed shuffle tree)
+        static_assert(T::kRegA % 2 == 0 && T::kFx >= 4 * NT, "sum buffer inside the face buffer");
+        double *sSum = reinterpret_cast<double *>(sFx);
+        sSum[tid] = mass;
+        sSum[NT + tid] = sed;
+        if ((tid & 31) == 0) sRed[tid >> 5] = (double)__uint_as_float(mb);
         __syncthreads();
-        if (tid == 0) {
-            double mm = sRed[0], ms = sRed[kWarps], sd = sRed[2 * kWarps];
-            for (int w = 1; w < kWarps; w++) {
-                mm = fmin(mm, sRed[w]);
-                ms += sRed[kWarps + w];
-                sd += sRed[2 * kWarps + w];
+        if (tid < 32) {
+            double ms = 0.0, sd = 0.0;
+            for (int k = tid; k < NT; k += 32) {
+                ms += sSum[k];
+                sd += sSum[NT + k];
             }
-            __stcg(A.partials + blin, mm);
-            __stcg(A.partials + nb + blin, ms);
-            __stcg(A.partials + 2 * nb + blin, sd);
-            __threadfence();
-            sLast = (atomicAdd(A.ticket, 1u) == nb - 1);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                ms += __shfl_xor_sync(0xffffffffu, ms, o);
+                sd += __shfl_xor_sync(0xffffffffu, sd, o);
+            }
+            if (tid == 0) {
+                double mm = sRed[0];
+                for (int w = 1; w < kWarps; w++) mm = fmin(mm, sRed[w]);
+                __stcg(A.partials + blin, mm);
+                __stcg(A.partials + nb + blin, ms);
+                __stcg(A.partials + 2 * nb + blin, sd);
+                __threadfence();
+                sLast = (atomicAdd(A.ticket, 1u) == nb - 1);
+            }
         }
         __syncthreads();
         if (sLast) {
@@ -722,10 +750,10 @@ Variant32 make_variant32() {
 
 // tile W x H / minimum resident CTAs per SM (register budget)
 const Variant32 *variants32(int *n) {
-    static Variant32 v[7] = {make_variant32<32, 8, 2>(),  make_variant32<16, 16, 2>(), make_variant32<32, 16, 1>(),
+    static Variant32 v[8] = {make_variant32<32, 8, 2>(),  make_variant32<16, 16, 2>(), make_variant32<32, 16, 1>(),
                              make_variant32<64, 4, 2>(),  make_variant32<32, 8, 3>(),  make_variant32<16, 16, 3>(),
-                             make_variant32<32, 8, 4>()};
-    if (n) *n = 7;
+                             make_variant32<32, 8, 4>(),  make_variant32<32, 16, 2>()};
+    if (n) *n = 8;
     return v;
 }
 
