@@ -170,12 +170,19 @@ __global__ void __launch_bounds__(TX *TY, MINB) stage64_kernel(Stage64Args A) {
         Vout = par ? A.bufA : A.bufB;
     }
 
+    // tile and halo inside the grid, not periodic: no clamping, and every
+    // edge of the tile is an interior edge
+    const bool inner = !periodic && x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= npx && y0 + TY + 2 <= npy;
+
     // ---- phase 1: tile + halo -> smem
     for (int idx = tid; idx < PS; idx += NT) {
-        int ly = idx / LX, lx = idx - ly * LX;
-        int gx = wrap_clamp(x0 + lx - 2, npx, periodic);
-        int gy = wrap_clamp(y0 + ly - 2, npy, periodic);
-        long long g = (long long)gy * pitch + gx;
+        const int ly = idx / LX, lx = idx - ly * LX;
+        int gx = x0 + lx - 2, gy = y0 + ly - 2;
+        if (!inner) {
+            gx = wrap_clamp(gx, npx, periodic);
+            gy = wrap_clamp(gy, npy, periodic);
+        }
+        const long long g = (long long)gy * pitch + gx;
 #pragma unroll
         for (int f = 0; f < 5; f++) sV[f * PS + idx] = Vin[f * plane + g];
         sM[idx] = A.mask[g];
@@ -253,7 +260,7 @@ __global__ void __launch_bounds__(TX *TY, MINB) stage64_kernel(Stage64Args A) {
     __syncthreads();
 
     // ---- phase 4: edges (each once per tile, one Riemann call site)
-    const bool series_on = P.read_files && (t < A.tCC[A.timeCC - 2]);
+    const bool series_on = !inner && P.read_files && (t < A.tCC[A.timeCC - 2]);
     constexpr int NV = (TX + 1) * TY, NH = TX * (TY + 1);
     constexpr int FS = TY * TX;  // flux plane stride; planes FL, FR, FD, FU
     for (int item = tid; item < NV + NH; item += NT) {
@@ -261,7 +268,30 @@ __global__ void __launch_bounds__(TX *TY, MINB) stage64_kernel(Stage64Args A) {
         int nx, ny, fixed, seg = 0;
         bool bnd = false, seam = false, vert;
         double *outM = nullptr, *outP = nullptr;
-        if (item < NV) {
+        if (inner) {  // interior edges only (uniform per tile): no bounds or boundary cases
+            if (item < NV) {
+                vert = true;
+                nx = 1;
+                ny = 0;
+                const int r = item / (TX + 1), e = item - r * (TX + 1);
+                a = get5(sFx + (5 * TY + r) * FXW + e, TY * FXW);
+                b = get5(sFx + r * FXW + (e + 1), TY * FXW);
+                fixed = (int)sM[(r + 2) * LX + e + 1] * (int)sM[(r + 2) * LX + e + 2];
+                if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
+                if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
+            } else {
+                vert = false;
+                nx = 0;
+                ny = 1;
+                const int it = item - NV;
+                const int e = it / TX, c = it - e * TX;
+                a = get5(sFy + (5 * FYH + e) * TX + c, FYH * TX);
+                b = get5(sFy + (e + 1) * TX + c, FYH * TX);
+                fixed = (int)sM[(e + 1) * LX + c + 2] * (int)sM[(e + 2) * LX + c + 2];
+                if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
+                if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
+            }
+        } else if (item < NV) {
             vert = true;
             const int r = item / (TX + 1), e = item - r * (TX + 1);
             const int ex = x0 + e, ey = y0 + r;
