@@ -121,24 +121,34 @@ class Clocks:
                 "reasons": sorted(reasons)}
 
 
-def dist_setup(n):
+def dist_setup(n, backend=None):
+    """One process per GPU (torchrun env).  Replicas only: the process group
+    carries the barrier around the timed region and the max over ranks of the
+    device time, never data.  backend: "nccl" (default) or "gloo" (CPU
+    tests of this plumbing)."""
     if n <= 1 or "RANK" not in os.environ:
         return 0, 1, int(os.environ.get("LOCAL_RANK", 0)), None
     import datetime
 
     import torch
     import torch.distributed as dist
+    backend = backend or os.environ.get("TSU_DIST_BACKEND", "nccl")
     local = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return dist.get_rank(), dist.get_world_size(), local, dist
+
+
+def _on_gpu(dist):
+    return dist.get_backend() == "nccl"
 
 
 def dist_max(dist, v, local):
     if dist is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda:%d" % local)
+    t = torch.tensor([v], dtype=torch.float64, device=("cuda:%d" % local) if _on_gpu(dist) else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -146,8 +156,11 @@ def dist_max(dist, v, local):
 def barrier(dist, local):
     if dist is not None:
         import torch
-        dist.barrier(device_ids=[local])
-        torch.cuda.synchronize(local)
+        if _on_gpu(dist):
+            dist.barrier(device_ids=[local])
+            torch.cuda.synchronize(local)
+        else:
+            dist.barrier()
 
 
 def cpu_baseline(max_seconds=20.0):

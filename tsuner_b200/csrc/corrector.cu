@@ -20,15 +20,18 @@
 // that starts inside the patch: core matrix = 8 consecutive pixels of one
 // tile row (16-byte rows), the two K chunks one plane apart (LBO = plane
 // size) and the 16 row groups one patch row apart (SBO = 160 B).  No im2col
-// copy is made.  CTAs are persistent; the patch and the TMEM accumulator are
-// double-buffered so that the load of tile i+1 and the epilogue of tile i-1
-// overlap the MMAs of tile i.
+// copy is made.  The patch arrives by TMA: four 4-D box loads per tile (one
+// per channel quarter, zero fill outside the image = the convolution's
+// padding) completing on an mbarrier.  CTAs are persistent; the patch and the
+// TMEM accumulator are double-buffered so that the load of tile i+1 and the
+// epilogue of tile i-1 overlap the MMAs of tile i.
 //
 // Weight gradient (conv3x3_wgrad_kernel): dW[cout][tap][cin] =
 //   sum_p dZ[p][cout] X[p + off(tap)][cin], a GEMM with the pixels as the
 // reduction dimension: D[288 (tap,cin) x 32 (cout)] in three M=128 blocks,
 // MN-major operands (8 pixels x 16 bytes per core matrix): A is copied from
-// the patch planes in 128-byte core matrices, B is the dZ tile itself.  Row
+// the patch planes in 128-byte core matrices, B is the dZ tile itself (both
+// loaded by TMA).  Row
 // 288 of A is all ones, so D[288][cout] is the bias gradient.  Each CTA
 // accumulates a strip of tiles in TMEM and adds its partial result to the
 // FP32 gradients with atomics.
@@ -36,6 +39,7 @@
 // Every mbarrier wait is bounded (globaltimer); on expiry the kernel sets
 // the error word, waits once more (bounded) for its MMAs, frees its TMEM and
 // returns.
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched from the driver at run time)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -58,13 +62,15 @@ constexpr int C = 32;                       // channels
 constexpr int TXP = 8, TYP = 16;            // output tile (128 pixels)
 constexpr int PW = TXP + 2, PH = TYP + 2;   // patch 10 x 18
 constexpr int PPIX = PW * PH;               // 180
-constexpr int kPlane = PPIX * 16;           // one channel-quarter plane: 2880 B
-constexpr int kPatch = 4 * kPlane;          // 11520 B
+constexpr int kPlaneData = PPIX * 16;       // one channel-quarter plane: 2880 B
+constexpr int kPlane = 2944;                // plane stride: 23 x 128 B (TMA destinations 128-byte aligned)
+constexpr int kPatch = 4 * kPlane;          // 11776 B
 constexpr int kWBytes = 9 * 4 * 32 * 16;    // weights: 18432 B
 constexpr int KROWS = 9 * C;                // 288
 constexpr unsigned long long kWaitNs = 500000000ull;  // 0.5 s per wait
 
 constexpr int kFwdSmem = 1024 + kWBytes + 2 * kPatch + 64;
+static_assert(kPlane % 128 == 0 && kPlane >= kPlaneData && kWBytes % 128 == 0, "TMA destinations");
 // wgrad: patch + dZ tile + A for half of the 8 K steps (4 x 3 M blocks x 4 KB);
 // ~67 KB, so three CTAs fit on an SM
 constexpr int kZPlane = 128 * 16;
@@ -167,6 +173,20 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src, int bytes
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// 4-D tiled TMA load (no multicast) into this CTA's shared memory, completing
+// `box bytes` of transactions on `bar`; coordinates (channel, x, y, image)
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
     __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<uint32_t *>(&h);
@@ -184,18 +204,14 @@ __host__ __device__ inline TileGeom tile_geom(int nimg, int H, int W) {
     return g;
 }
 
-// 10 x 18 x 32 input patch (zero padding) -> four channel-quarter planes
-__device__ __forceinline__ void load_patch(const bf16 *__restrict__ X, int img, int H, int W, int x0, int y0,
-                                           unsigned char *patch, int tid) {
-    const bf16 *Xi = X + (long long)img * H * W * C;
-    for (int c = tid; c < PPIX * 4; c += 128) {
-        const int pix = c >> 2, q = c & 3;
-        const int pr = pix / PW, pc = pix - pr * PW;
-        const int gy = y0 + pr - 1, gx = x0 + pc - 1;
-        const bool in = gy >= 0 && gy < H && gx >= 0 && gx < W;
-        const bf16 *src = in ? Xi + ((long long)gy * W + gx) * C + q * 8 : Xi;
-        cp_async16(patch + q * kPlane + pix * 16, src, in ? 16 : 0);
-    }
+// 10 x 18 x 32 input patch (zero fill outside the image) -> four
+// channel-quarter planes: one TMA box (8 channels x 10 x 18) per plane.  The
+// innermost coordinate (channel 8q) is a multiple of 16 bytes; the halo may
+// start at x0 - 1 = -1 or y0 - 1 = -1, which loads zeros.
+__device__ __forceinline__ void issue_patch(const CUtensorMap *map, int img, int x0, int y0, unsigned char *patch,
+                                            uint64_t *bar) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) tma_load_4d(patch + q * kPlane, map, 8 * q, x0 - 1, y0 - 1, img, bar);
 }
 
 struct ConvArgs {
@@ -252,13 +268,14 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs &a, const TileGeom 
     }
 }
 
-__global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a) {
+__global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __grid_constant__ CUtensorMap tmX) {
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
     unsigned char *sW = sm;
     unsigned char *sP[2] = {sm + kWBytes, sm + kWBytes + kPatch};
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + kWBytes + 2 * kPatch);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + kWBytes + 2 * kPatch);  // [2] MMA done, [2] patch loaded
+    uint64_t *full = mbar + 2;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 4);
     __shared__ float sBias[32];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TileGeom G = tile_geom(a.nimg, a.H, a.W);
@@ -272,10 +289,11 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a) {
     if (tid < 32) sBias[tid] = a.bias ? a.bias[tid] : 0.f;
     if (warp == 0) tmem_alloc(tslot, 64);
     if (tid == 0) {
-        mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
+        for (int k = 0; k < 4; k++) mbar_init(&mbar[k], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    cp_async_wait_all();  // the weights
+    fence_async_smem();
     fence_before();
     __syncthreads();
     fence_after();
@@ -284,14 +302,15 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a) {
     const uint32_t w_u32 = smem_u32(sW);
 
     bool failed = false;
-    int prev = -1, i = 0;
+    int prev = -1, i = 0, last_load = -1;
     for (int t = blockIdx.x;; t += gridDim.x, i++) {
         const bool have = t < G.total;
-        if (have) {
+        if (have && tid == 0) {  // the patch buffer's previous MMAs finished (waited below one tile ago)
             const int img = t / G.per_img, r = t - img * G.per_img;
             const int tyi = r / G.ntx, txi = r - tyi * G.ntx;
-            load_patch(a.X, img, a.H, a.W, txi * TXP, tyi * TYP, sP[i & 1], tid);
-            cp_async_commit();
+            mbar_expect_tx(&full[i & 1], 4 * kPlaneData);
+            issue_patch(&tmX, img, txi * TXP, tyi * TYP, sP[i & 1], &full[i & 1]);
+            last_load = i;
         }
         if (prev >= 0) {  // epilogue of the previous tile overlaps this tile's loads
             const int j = i - 1;
@@ -304,12 +323,10 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a) {
             conv_epilogue(a, G, prev, tmem + (uint32_t)((j & 1) * 32), warp, lane, sBias);
         }
         if (!have) break;
-        cp_async_wait_all();
-        fence_async_smem();
         fence_before();
         __syncthreads();
         fence_after();
-        if (tid == 0) {
+        if (tid == 0 && mbar_wait(&full[i & 1], (i >> 1) & 1)) {
             const uint32_t p_u32 = smem_u32(sP[i & 1]);
             const uint32_t d = tmem + (uint32_t)((i & 1) * 32);
 #pragma unroll 1
@@ -327,10 +344,12 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a) {
         prev = t;
     }
     if (failed) {
-        if (tid == 0) atomicExch(&g_corr_err, 1);
-        // the copies of this tile and the MMAs of the last issued tile may
-        // still run: wait for them once more
-        cp_async_wait_all();
+        if (tid == 0) {
+            atomicExch(&g_corr_err, 1);
+            // the patch load of this tile may still run: wait for it once more
+            if (last_load >= 0) mbar_wait(&full[last_load & 1], (last_load >> 1) & 1);
+        }
+        // the MMAs of the last issued tile may still run
         mbar_wait(&mbar[(i - 1) & 1], ((i - 1) >> 1) & 1);
     }
     fence_before();
@@ -341,15 +360,16 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a) {
 
 // Weight (and bias) gradient, accumulated into dW[cout][288] and db[32].
 __global__ void __launch_bounds__(128, kWgCtasPerSm)
-    conv3x3_wgrad_kernel(const bf16 *__restrict__ X, const bf16 *__restrict__ dZ, int nimg, int H, int W,
-                         float *__restrict__ dW, float *__restrict__ db) {
+    conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmZ, int nimg,
+                         int H, int W, float *__restrict__ dW, float *__restrict__ db) {
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
     unsigned char *sP = sm;
     unsigned char *sZ = sm + kPatch;
     unsigned char *sA = sZ + 4 * kZPlane;
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(sA + kWgHalf * 3 * kABlock);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sA + kWgHalf * 3 * kABlock);  // MMA done
+    uint64_t *full = mbar + 1;                                                   // tile loaded
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TileGeom G = tile_geom(nimg, H, W);
 
@@ -364,6 +384,7 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
     if (warp == 0) tmem_alloc(tslot, 128);
     if (tid == 0) {
         mbar_init(mbar, 1);
+        mbar_init(full, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     fence_before();
@@ -379,18 +400,21 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
         const int img = t / G.per_img, r = t - img * G.per_img;
         const int tyi = r / G.ntx, txi = r - tyi * G.ntx;
         const int x0 = txi * TXP, y0 = tyi * TYP;
-        load_patch(X, img, H, W, x0, y0, sP, tid);
-        const bf16 *Zi = dZ + (long long)img * H * W * C;
-        for (int c = tid; c < 128 * 4; c += 128) {
-            const int m = c >> 2, q = c & 3, px = m & 7, py = m >> 3;
-            const int gx = x0 + px, gy = y0 + py;
-            const bool in = gx < W && gy < H;
-            const bf16 *src = in ? Zi + ((long long)gy * W + gx) * C + q * 8 : Zi;
-            cp_async16(sZ + q * kZPlane + m * 16, src, in ? 16 : 0);
+        if (tid == 0) {  // patch (4 x 2880 B) and the dZ tile (4 x 8 x 16 x 8 channels) by TMA
+            mbar_expect_tx(full, 4 * kPlaneData + 4 * kZPlane);
+            issue_patch(&tmX, img, x0, y0, sP, full);
+#pragma unroll
+            for (int q = 0; q < 4; q++) tma_load_4d(sZ + q * kZPlane, &tmZ, 8 * q, x0, y0, img, full);
         }
-        cp_async_commit();
-        cp_async_wait_all();
-        __syncthreads();
+        const bool loaded = mbar_wait(full, i & 1);
+        if (__syncthreads_or(!loaded)) {
+            failed = true;
+            if (tid == 0) {
+                atomicExch(&g_corr_err, 1);
+                mbar_wait(full, i & 1);
+            }
+            break;
+        }
         // two rounds of 4 K steps (tile rows 0-7, then 8-15)
         for (int hh = 0; hh < 2 && !failed; hh++) {
             // A core matrices (s, G = tap*4 + quarter, kgroup): 8 pixels of
@@ -578,6 +602,37 @@ __global__ void apply_kernel(const float *__restrict__ Y, const float *__restric
     }
 }
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encoder() {
+    static EncodeTiledFn f = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return f;
+}
+
+// tensor map of an NHWC BF16 32-channel tensor [nimg][H][W][32] with boxes of
+// 8 channels x bx x by pixels
+cudaError_t make_map(CUtensorMap *m, const void *base, int nimg, int H, int W, int bx, int by) {
+    EncodeTiledFn f = encoder();
+    if (!f) return cudaErrorNotSupported;
+    const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)nimg};
+    const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)C * 2 * W, (cuuint64_t)C * 2 * W * H};
+    const cuuint32_t box[4] = {8, (cuuint32_t)bx, (cuuint32_t)by, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    const CUresult r = f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 cudaError_t prepare() {
     static bool done = false;
     if (done) return cudaSuccess;
@@ -601,18 +656,27 @@ int num_sms() {
 cudaError_t conv_launch(const ConvArgs &a, cudaStream_t st) {
     cudaError_t e = prepare();
     if (e != cudaSuccess) return e;
+    if (reinterpret_cast<uintptr_t>(a.X) % 16) return cudaErrorInvalidValue;
+    CUtensorMap mx;
+    e = make_map(&mx, a.X, a.nimg, a.H, a.W, PW, PH);
+    if (e != cudaSuccess) return e;
     const TileGeom G = tile_geom(a.nimg, a.H, a.W);
     const int ctas = std::min(G.total, 4 * num_sms());
-    conv3x3_fwd_kernel<<<ctas, 128, kFwdSmem, st>>>(a);
+    conv3x3_fwd_kernel<<<ctas, 128, kFwdSmem, st>>>(a, mx);
     return cudaGetLastError();
 }
 
 cudaError_t wgrad_launch(const bf16 *X, const bf16 *dZ, int nimg, int H, int W, float *dW, float *db, cudaStream_t st) {
     cudaError_t e = prepare();
     if (e != cudaSuccess) return e;
+    if (reinterpret_cast<uintptr_t>(X) % 16 || reinterpret_cast<uintptr_t>(dZ) % 16) return cudaErrorInvalidValue;
+    CUtensorMap mx, mz;
+    e = make_map(&mx, X, nimg, H, W, PW, PH);
+    if (e == cudaSuccess) e = make_map(&mz, dZ, nimg, H, W, TXP, TYP);
+    if (e != cudaSuccess) return e;
     const TileGeom G = tile_geom(nimg, H, W);
     const int ctas = std::min(G.total, kWgCtasPerSm * num_sms());
-    conv3x3_wgrad_kernel<<<ctas, 128, kWgSmem, st>>>(X, dZ, nimg, H, W, dW, db);
+    conv3x3_wgrad_kernel<<<ctas, 128, kWgSmem, st>>>(mx, mz, nimg, H, W, dW, db);
     return cudaGetLastError();
 }
 
