@@ -403,8 +403,13 @@ def run_ours(a, rank, world, local, dist):
         wet = V64[0] > w.p.epsilon_h
         dh = V_prim[0] - V64[0]
         m64 = float(V64[0].sum())
+        hbm64, kind64 = peaks()
+        ach64 = BYTES_PER_CELL_STEP["f64"] * n * a.steps / (ms64 / 1e3) / 1e9
         other = {"fp64_plain": {"value": round(world * n * a.steps / (ms64 / 1e3) / 1e6, 3),
-                                "unit": "Mcell-steps/s", "ms_per_step": round(ms64 / a.steps, 4)},
+                                "unit": "Mcell-steps/s", "ms_per_step": round(ms64 / a.steps, 4),
+                                "roofline": {"bound": "hbm", "achieved": round(ach64, 1), "peak": hbm64,
+                                             "unit": "GB/s", "frac": round(ach64 / hbm64, 4), "peak_kind": kind64,
+                                             "bytes_per_cell_step": BYTES_PER_CELL_STEP["f64"]}},
                  "fp32_vs_fp64": {"steps": a.warmup + a.steps,
                                   "linf_depth_m": float(np.abs(dh).max()),
                                   "l2_depth_m": float(np.sqrt(np.mean(dh[wet] ** 2))) if wet.any() else 0.0,
