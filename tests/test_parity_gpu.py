@@ -14,6 +14,8 @@ Bars, per field after the run:
     flags (h > epsilon_h) identical, same step count.  Its link-time code
     generation rounds differently in the last bits (measured <= 3.2e-15).
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -203,6 +205,18 @@ def test_config2_slice_4096_vs_reference_build():
     (its link-time code generation rounds differently), so it is held to 1e-10."""
     w = W.nwave_shelf(4096, 4096, 5.0)
     ref_vs_new(w, 40, "default", w.sw, recipe_tol=1e-10)
+
+
+@need_ref
+@pytest.mark.skipif(os.environ.get("TSU_FULL_CONFIGS") != "1",
+                    reason="full-size run (~4 min): set TSU_FULL_CONFIGS=1")
+def test_config2_full_5000_steps_vs_reference_build():
+    """The whole shelf configuration: 4096^2, N-wave series, harbour mask,
+    5000 steps (t = 195.27 s).  Value-identical to the -nolto reference build;
+    the recipe build within 1e-12 relative per field (measured on a B200:
+    8.9e-13 in qx, 2.8e-15 in h; wet/dry flags identical)."""
+    w = W.nwave_shelf(4096, 4096, 5.0)
+    ref_vs_new(w, 5000, "default", w.sw, recipe_tol=1e-12)
 
 
 @pytest.mark.parametrize("variant,sw", [
