@@ -39,7 +39,6 @@
 // Every mbarrier wait is bounded (globaltimer); on expiry the kernel sets
 // the error word, waits once more (bounded) for its MMAs, frees its TMEM and
 // returns.
-#include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched from the driver at run time)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -51,6 +50,7 @@
 #include <new>
 #include <vector>
 
+#include "async.cuh"
 #include "tsuner_b200.h"
 
 namespace tsu {
@@ -67,7 +67,6 @@ constexpr int kPlane = 2944;                // plane stride: 23 x 128 B (TMA des
 constexpr int kPatch = 4 * kPlane;          // 11776 B
 constexpr int kWBytes = 9 * 4 * 32 * 16;    // weights: 18432 B
 constexpr int KROWS = 9 * C;                // 288
-constexpr unsigned long long kWaitNs = 500000000ull;  // 0.5 s per wait
 
 constexpr int kFwdSmem = 1024 + kWBytes + 2 * kPatch + 64;
 constexpr int kFwdCtasPerSm = 5;  // 5 x (43 KB + 1 KB) of shared memory, 5 x 64 TMEM columns
@@ -83,16 +82,6 @@ constexpr int kWgCtasPerSm = 3;
 
 __device__ int g_corr_err;  // set by a kernel whose wait expired
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ unsigned long long gtimer() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
 // UMMA shared-memory descriptor, no swizzle, sm100 version field
 __device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
     return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
@@ -105,26 +94,6 @@ __host__ __device__ constexpr uint32_t idesc(int M, int N, int a_mn, int b_mn) {
            ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint64_t *bar, unsigned parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
-    const unsigned long long t0 = gtimer();
-    while (!mbar_try(bar, parity))
-        if (gtimer() - t0 > kWaitNs) return false;
-    return true;
-}
 __device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
                  "r"(ncols)
@@ -136,7 +105,6 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 }
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t id, uint32_t accum) {
     asm volatile(
@@ -174,20 +142,6 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src, int bytes
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-// 4-D tiled TMA load (no multicast) into this CTA's shared memory, completing
-// `box bytes` of transactions on `bar`; coordinates (channel, x, y, image)
-__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
-                                            uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-        "[%6];" ::"r"(smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
-        : "memory");
-}
 
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
     __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
@@ -292,7 +246,7 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __gr
     if (warp == 0) tmem_alloc(tslot, 64);
     if (tid == 0) {
         for (int k = 0; k < 4; k++) mbar_init(&mbar[k], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_init_fence();
     }
     cp_async_wait_all();  // the weights
     fence_async_smem();
@@ -387,7 +341,7 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
     if (tid == 0) {
         mbar_init(mbar, 1);
         mbar_init(full, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        mbar_init_fence();
     }
     fence_before();
     __syncthreads();
@@ -604,26 +558,10 @@ __global__ void apply_kernel(const float *__restrict__ Y, const float *__restric
     }
 }
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encoder() {
-    static EncodeTiledFn f = [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            p = nullptr;
-        return reinterpret_cast<EncodeTiledFn>(p);
-    }();
-    return f;
-}
-
 // tensor map of an NHWC BF16 32-channel tensor [nimg][H][W][32] with boxes of
 // 8 channels x bx x by pixels
 cudaError_t make_map(CUtensorMap *m, const void *base, int nimg, int H, int W, int bx, int by) {
-    EncodeTiledFn f = encoder();
+    EncodeTiledFn f = tensor_map_encoder();
     if (!f) return cudaErrorNotSupported;
     const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)nimg};
     const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)C * 2 * W, (cuuint64_t)C * 2 * W * H};

@@ -222,6 +222,9 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
     if (e == cudaSuccess) e = consts_launch(s->p, s->dconsts, s->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&s->hconsts, s->dconsts, sizeof(TsuConsts), cudaMemcpyDeviceToHost, s->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    if (e == cudaSuccess && !s->fp32)
+        s->tma = stage64_tma_maps((const double *)s->A, (const double *)s->B, s->pitch, s->plane, p->npx, p->npy,
+                                  &s->tmA, &s->tmB);
     if (e != cudaSuccess) {
         int r = cuda_fail(e, "tsu_create");
         free_all(s);
@@ -340,6 +343,9 @@ Stage64Args TsuSolver::args() const {
     a.pitch = pitch;
     a.plane = plane;
     a.phys = phys;
+    a.tmA = tmA;
+    a.tmB = tmB;
+    a.tma = tma ? 1 : 0;
     return a;
 }
 
@@ -442,11 +448,22 @@ extern "C" int tsu_step(TsuSolver *s, long nsteps) {
     return TSU_OK;
 }
 
+// TSU_ERR_CUDA if a kernel recorded an expired bounded wait (SC_ERR)
+static int device_wait_error(TsuSolver *s) {
+    double flag = 0.0;
+    CK(cudaMemcpy(&flag, s->scal + SC_ERR, sizeof(double), cudaMemcpyDeviceToHost));
+    if (flag != 0.0) {
+        snprintf(g_err, sizeof(g_err), "a bounded wait for a tile load expired on the device");
+        return TSU_ERR_CUDA;
+    }
+    return TSU_OK;
+}
+
 extern "C" int tsu_sync(TsuSolver *s) {
     if (!s) return TSU_ERR_INVALID;
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->st));
-    return TSU_OK;
+    return device_wait_error(s);
 }
 
 extern "C" int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *steps_done) {
@@ -537,7 +554,7 @@ extern "C" int tsu_get_time(TsuSolver *s, double *t, double *dt, long *steps) {
     if (t) *t = sc[SC_T];
     if (dt) *dt = sc[SC_DT];
     if (steps) *steps = (long)sc[SC_STEPS];
-    return TSU_OK;
+    return device_wait_error(s);
 }
 
 extern "C" int tsu_get_sums(TsuSolver *s, double *water, double *sediment) {

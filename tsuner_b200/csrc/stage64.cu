@@ -30,6 +30,7 @@
 #include <cstring>
 
 #include "physics64.cuh"
+#include "async.cuh"
 #include "stage64.h"
 
 namespace tsu {
@@ -47,7 +48,8 @@ struct Tile {
     static constexpr int kRegA = (kSV + kSUC) > kFlux ? (kSV + kSUC) : kFlux;
     static constexpr int kFx = 10 * TY * FXW, kFy = 10 * FYH * TX, kDeta = 2 * TY * TX, kRed = NT / 32;
     static constexpr int kDoubles = kRegA + kFx + kFy + kDeta + kRed;
-    static constexpr size_t smem() { return sizeof(double) * kDoubles + PS + 16; }
+    // + 128: the base is rounded up to 128 bytes (TMA destination)
+    static constexpr size_t smem() { return sizeof(double) * kDoubles + PS + 16 + 128; }
 };
 
 __device__ __forceinline__ int wrap_clamp(int g, int n, bool periodic) {
@@ -134,10 +136,12 @@ __device__ __forceinline__ void put5a(double *base, int stride, const double D[5
 }
 
 template <int TX, int TY, int NTHR, int MINB, int ORDER, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(Stage64Args A) {
+__global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_constant__ Stage64Args A) {
     using T = Tile<TX, TY, NTHR>;
     constexpr int NT = T::NT, LX = T::LX, LY = T::LY, PS = T::PS, FXW = T::FXW, FYH = T::FYH;
-    extern __shared__ __align__(16) double smem[];
+    extern __shared__ __align__(16) double smem_raw[];
+    double *smem = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    __shared__ uint64_t sBar;  // the tile's TMA load
     const Phys64 &P = A.phys;
     double *sV = smem;                  // [5][LY][LX]
     double *sUC = smem + T::kSV;        // [3][LY][LX]  (ux, uy, c)
@@ -178,18 +182,34 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(Stage64Args A) {
     // edge of the tile is an interior edge
     const bool inner = !periodic && x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= npx && y0 + TY + 2 <= npy;
 
-    // ---- phase 1: tile + halo -> smem
-    for (int idx = tid; idx < PS; idx += NT) {
-        const int ly = idx / LX, lx = idx - ly * LX;
-        int gx = x0 + lx - 2, gy = y0 + ly - 2;
-        if (!inner) {
-            gx = wrap_clamp(gx, npx, periodic);
-            gy = wrap_clamp(gy, npy, periodic);
+    // ---- phase 1: tile + halo -> smem.  Interior tiles: one TMA box of the
+    // 5 state planes (x0 - 2 doubles = a multiple of 16 bytes); the mask and
+    // boundary tiles (clamped or wrapped halo) with ordinary loads.
+    const bool use_tma = inner && A.tma;
+    if (use_tma) {
+        if (tid == 0) {
+            mbar_init(&sBar, 1);
+            mbar_init_fence();
+            mbar_expect_tx(&sBar, 5 * PS * sizeof(double));
+            tma_load_3d(sV, (Vin == A.bufB) ? &A.tmB : &A.tmA, x0 - 2, y0 - 2, 0, &sBar);
         }
-        const long long g = (long long)gy * pitch + gx;
+        for (int idx = tid; idx < PS; idx += NT) {
+            const int ly = idx / LX, lx = idx - ly * LX;
+            sM[idx] = A.mask[(long long)(y0 + ly - 2) * pitch + (x0 + lx - 2)];
+        }
+    } else {
+        for (int idx = tid; idx < PS; idx += NT) {
+            const int ly = idx / LX, lx = idx - ly * LX;
+            int gx = x0 + lx - 2, gy = y0 + ly - 2;
+            if (!inner) {
+                gx = wrap_clamp(gx, npx, periodic);
+                gy = wrap_clamp(gy, npy, periodic);
+            }
+            const long long g = (long long)gy * pitch + gx;
 #pragma unroll
-        for (int f = 0; f < 5; f++) sV[f * PS + idx] = Vin[f * plane + g];
-        sM[idx] = A.mask[g];
+            for (int f = 0; f < 5; f++) sV[f * PS + idx] = Vin[f * plane + g];
+            sM[idx] = A.mask[g];
+        }
     }
     const bool cell_thread = tid < TX * TY;  // owns a cell in the update
     const int tx = cell_thread ? tid % TX : 0, ty = cell_thread ? tid / TX : 0;
@@ -202,6 +222,16 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(Stage64Args A) {
         for (int f = 0; f < 5; f++) v0[f] = V0[f * plane + gown];
     }
     __syncthreads();
+    if (use_tma) {  // every thread sees the box land (bounded wait)
+        const bool ok = mbar_wait(&sBar, 0);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                A.scal[SC_ERR] = 1.0;
+                mbar_wait(&sBar, 0);
+            }
+            return;
+        }
+    }
 
     const int cidx = (ty + 2) * LX + (tx + 2);
     double vc[5];
@@ -581,6 +611,18 @@ __global__ void consts_kernel(SimParams p, TsuConsts *k) {
 }
 
 // ------------------------------------------------------------------ host side
+EncodeTiledFn tensor_map_encoder() {
+    static EncodeTiledFn f = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return f;
+}
+
 namespace {
 
 struct Variant {
@@ -633,6 +675,26 @@ cudaError_t stage64_prepare() {
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+bool stage64_tma_maps(const double *bufA, const double *bufB, long long pitch, long long plane, int npx, int npy,
+                      CUtensorMap *tmA, CUtensorMap *tmB) {
+    EncodeTiledFn f = tensor_map_encoder();
+    const Variant &v = variant();
+    if (!f || npx < v.tx + 4 || npy < v.ty + 4) return false;
+    if (reinterpret_cast<uintptr_t>(bufA) % 16 || reinterpret_cast<uintptr_t>(bufB) % 16) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)npx, (cuuint64_t)npy, 5};
+    const cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(double), (cuuint64_t)plane * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)(v.tx + 4), (cuuint32_t)(v.ty + 4), 5};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const double *bufs[2] = {bufA, bufB};
+    CUtensorMap *maps[2] = {tmA, tmB};
+    for (int k = 0; k < 2; k++)
+        if (f(maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(bufs[k]), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    return true;
 }
 
 dim3 stage64_grid(int npx, int npy) {

@@ -1,5 +1,6 @@
 // stage64.h -- launch interface of the FP64 fused stage kernels.
 #pragma once
+#include <cuda.h>  // CUtensorMap
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
@@ -20,9 +21,15 @@ namespace tsu {
 //   [3] steps taken           [4] order-1 ping-pong parity
 //   [5] FP32 form: sum of water depth after the last step (FP64)
 //   [6] FP32 form: sum of H + hc after the last step (FP64)
-enum { SC_T = 0, SC_DT = 1, SC_TEND = 2, SC_STEPS = 3, SC_PAR = 4, SC_MASS = 5, SC_SED = 6, SC_N = 8 };
+//   [7] non-zero when a bounded device wait expired (reported by the host)
+enum { SC_T = 0, SC_DT = 1, SC_TEND = 2, SC_STEPS = 3, SC_PAR = 4, SC_MASS = 5, SC_SED = 6, SC_ERR = 7, SC_N = 8 };
 
 struct Stage64Args {
+    // TMA descriptors of the two state buffers as 3-D tensors [5][npy][npx]
+    // (boxes = the loaded tile with its halo); used for tiles whose halo lies
+    // inside the grid when `tma` is set
+    CUtensorMap tmA, tmB;
+    int tma;
     double *bufA;           // U^n at step entry (and U^{n+1} at exit, order 2)
     double *bufB;           // U* (order 2) / ping-pong partner (order 1)
     const unsigned char *mask;
@@ -55,5 +62,10 @@ cudaError_t initial_dt_launch(const double *V, long long pitch, long long plane,
 cudaError_t fill_launch(double *p, long long n, double v, cudaStream_t st);
 cudaError_t consts_launch(const SimParams &p, TsuConsts *k, cudaStream_t st);
 size_t partials_needed(int npx, int npy);
+// encodes the TMA descriptors of the two FP64 state buffers for the current
+// tile shape; false if the driver cannot (the kernels then load with
+// ordinary instructions)
+bool stage64_tma_maps(const double *bufA, const double *bufB, long long pitch, long long plane, int npx, int npy,
+                      CUtensorMap *tmA, CUtensorMap *tmB);
 
 }  // namespace tsu
