@@ -16,6 +16,16 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// p advanced to the next multiple of ALIGN bytes of the shared window.  The
+// pad is added to the pointer (not computed through an integer round trip),
+// so the compiler still knows it addresses shared memory and keeps its
+// accesses shared-memory instructions.
+template <int ALIGN, typename T>
+__device__ __forceinline__ T *smem_align(T *p) {
+    const uint32_t pad = (ALIGN - (smem_u32(p) & (ALIGN - 1))) & (ALIGN - 1);
+    return reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(p) + pad);
+}
+
 __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

@@ -31,8 +31,8 @@
 // reduction dimension: D[288 (tap,cin) x 32 (cout)] in three M=128 blocks,
 // MN-major operands (8 pixels x 16 bytes per core matrix): A is copied from
 // the patch planes in 128-byte core matrices, B is the dZ tile itself (both
-// loaded by TMA).  Row
-// 288 of A is all ones, so D[288][cout] is the bias gradient.  Each CTA
+// loaded by TMA).  Row 288 of A is all ones, so D[288][cout] is the bias
+// gradient.  Each CTA
 // accumulates a strip of tiles in TMEM and adds its partial result to the
 // FP32 gradients with atomics.
 //
@@ -226,7 +226,7 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs &a, const TileGeom 
 
 __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __grid_constant__ CUtensorMap tmX) {
     extern __shared__ unsigned char sm_raw[];
-    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char *sm = smem_align<1024>(sm_raw);
     unsigned char *sW = sm;
     unsigned char *sP[2] = {sm + kWBytes, sm + kWBytes + kPatch};
     uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + kWBytes + 2 * kPatch);  // [2] MMA done, [2] patch loaded
@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
     conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmZ, int nimg,
                          int H, int W, float *__restrict__ dW, float *__restrict__ db) {
     extern __shared__ unsigned char sm_raw[];
-    unsigned char *sm = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char *sm = smem_align<1024>(sm_raw);
     unsigned char *sP = sm;
     unsigned char *sZ = sm + kPatch;
     unsigned char *sA = sZ + 4 * kZPlane;

@@ -222,9 +222,14 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
     if (e == cudaSuccess) e = consts_launch(s->p, s->dconsts, s->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&s->hconsts, s->dconsts, sizeof(TsuConsts), cudaMemcpyDeviceToHost, s->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
-    if (e == cudaSuccess && !s->fp32)
-        s->tma = stage64_tma_maps((const double *)s->A, (const double *)s->B, s->pitch, s->plane, p->npx, p->npy,
-                                  &s->tmA, &s->tmB);
+    // TSU_STAGE_TMA=0 makes every tile load with ordinary instructions
+    const char *tma_env = std::getenv("TSU_STAGE_TMA");
+    const bool tma_allowed = !(tma_env && tma_env[0] == '0');
+    if (e == cudaSuccess && tma_allowed)
+        s->tma = s->fp32 ? stage32_tma_maps((const float *)s->A, (const float *)s->B, s->pitch, s->plane, p->npx,
+                                            p->npy, &s->tmA, &s->tmB)
+                         : stage64_tma_maps((const double *)s->A, (const double *)s->B, s->pitch, s->plane, p->npx,
+                                            p->npy, &s->tmA, &s->tmB);
     if (e != cudaSuccess) {
         int r = cuda_fail(e, "tsu_create");
         free_all(s);
@@ -406,8 +411,12 @@ extern "C" int tsu_reset(TsuSolver *s) {
 int TsuSolver::launch_steps(long n) {
     if (fp32) {
         Stage32Args a = args32();
+        Tma32 tm;
+        tm.a = tmA;
+        tm.b = tmB;
+        tm.on = tma ? 1 : 0;
         for (long i = 0; i < n; i++)
-            for (int k = 0; k < sw.order; k++) CK(stage32_launch(sw.order, k, a, st));
+            for (int k = 0; k < sw.order; k++) CK(stage32_launch(sw.order, k, a, tm, st));
     } else {
         Stage64Args a = args();
         for (long i = 0; i < n; i++)

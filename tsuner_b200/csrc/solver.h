@@ -34,7 +34,7 @@ struct TsuSolver {
     cudaGraphExec_t graph_exec = nullptr;
     long last_launches = 0;
     bool has_state = false, ready = false, timed = false;
-    // FP64 form: TMA descriptors of A and B (interior tiles stage by TMA)
+    // TMA descriptors of A and B (interior tiles stage their loads by TMA)
     CUtensorMap tmA{}, tmB{};
     bool tma = false;
 

@@ -14,15 +14,20 @@
 
 #include <cstdlib>
 
+#include "async.cuh"
 #include "physics32.cuh"
 #include "stage32.h"
 
 namespace tsu {
 
+// Tile of TX x TY cells with a 2-cell halo.  In shared memory a row holds
+// the HX = 4 cells left of the tile (so that a row starts at x0 - 4, a
+// 16-byte aligned TMA coordinate for floats), the tile and 4 cells right of
+// it; only the 2 halo cells on each side (LXC = TX + 4 columns) are used.
 template <int TX_, int TY_>
 struct T32 {
     static constexpr int TX = TX_, TY = TY_, NT = TX * TY;
-    static constexpr int LX = TX + 4, LY = TY + 4, PS = LX * LY;
+    static constexpr int HX = 4, LXC = TX + 4, LX = TX + 2 * HX, LY = TY + 4, PS = LX * LY, PSC = LXC * LY;
     static constexpr int FXW = TX + 2, FYH = TY + 2;
     // per loaded cell: z, H, qx, qy, hc (loaded) + h, ux, uy, c (derived)
     static constexpr int kSV = 9 * PS, kFlux = 20 * TY * TX;
@@ -30,7 +35,8 @@ struct T32 {
     static constexpr int kFx = 12 * TY * FXW, kFy = 12 * FYH * TX;  // 2 faces x 6 floats
     static constexpr int kDeta = 2 * TY * TX, kWarps = NT / 32;
     static constexpr int kFloats = kRegA + kFx + kFy + kDeta;
-    static constexpr size_t smem() { return sizeof(float) * kFloats + sizeof(double) * 3 * kWarps + PS + 64; }
+    // + 128: the base is rounded up to 128 bytes (TMA destination)
+    static constexpr size_t smem() { return sizeof(float) * kFloats + sizeof(double) * 3 * kWarps + PS + 64 + 128; }
 };
 
 __device__ __forceinline__ int wrap_clamp32(int g, int n, bool periodic) {
@@ -117,11 +123,15 @@ __device__ __forceinline__ void recon32(const Phys32 &P, const float *s, int c, 
 // tile and number of tiles of this grid (for the end-of-step reduction).
 // P: the grid's physical parameters (A.phys, or the ensemble's shared
 // parameters with this member's grid fields).
+// tm: TMA descriptors of the state buffers (single grid), or null (ensemble).
 template <int TX, int TY, int ORDER, bool FIRST, bool LAST>
-__device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 &P, int bx, int by, unsigned blin,
-                                             unsigned nb, float *smem32) {
+__device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 &P, const Tma32 *tm, int bx, int by,
+                                             unsigned blin, unsigned nb, float *smem_raw) {
     using T = T32<TX, TY>;
     constexpr int NT = T::NT, LX = T::LX, PS = T::PS, FXW = T::FXW, FYH = T::FYH, kWarps = T::kWarps;
+    constexpr int HX = T::HX, LXC = T::LXC, PSC = T::PSC;
+    float *smem32 = smem_align<128>(smem_raw);
+    __shared__ uint64_t sBar;  // the tile's TMA load
     float *sV = smem32;
     float *sFlux = smem32;
     float *sFx = smem32 + T::kRegA;
@@ -164,17 +174,31 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     // edge of the tile is an interior edge
     const bool inner = !periodic && x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= npx && y0 + TY + 2 <= npy;
 
-    // ---- phase 1: load z, H, qx, qy, hc (+mask) with a 2-cell halo
-    for (int idx = tid; idx < PS; idx += NT) {
-        const int ly = idx / LX, lx = idx - ly * LX;
-        int gx = x0 + lx - 2, gy = y0 + ly - 2;
+    // ---- phase 1: load z, H, qx, qy, hc (+mask) with a 2-cell halo.  With
+    // descriptors, a tile whose 4-cell x-halo lies inside the grid stages the
+    // 5 planes with one TMA box (origin x0 - 4: a multiple of 16 bytes); the
+    // mask and the other tiles use ordinary loads of the needed cells.
+    const bool use_tma =
+        tm && tm->on && !periodic && x0 >= HX && y0 >= 2 && x0 + TX + HX <= npx && y0 + TY + 2 <= npy;
+    if (use_tma && tid == 0) {
+        mbar_init(&sBar, 1);
+        mbar_init_fence();
+        mbar_expect_tx(&sBar, 5 * PS * sizeof(float));
+        tma_load_3d(sV, (Vin == A.bufB) ? &tm->b : &tm->a, x0 - HX, y0 - 2, 0, &sBar);
+    }
+    for (int k = tid; k < PSC; k += NT) {
+        const int ly = k / LXC, lxc = k - ly * LXC;
+        const int idx = ly * LX + lxc + (HX - 2);
+        int gx = x0 + lxc - 2, gy = y0 + ly - 2;
         if (!inner) {
             gx = wrap_clamp32(gx, npx, periodic);
             gy = wrap_clamp32(gy, npy, periodic);
         }
         const long long g = (long long)gy * pitch + gx;
+        if (!use_tma) {
 #pragma unroll
-        for (int f = 0; f < 5; f++) sV[f * PS + idx] = __ldg(Vin + f * plane + g);
+            for (int f = 0; f < 5; f++) sV[f * PS + idx] = __ldg(Vin + f * plane + g);
+        }
         sM[idx] = __ldg(A.mask + g);
     }
     const int tx = tid % TX, ty = tid / TX;
@@ -193,7 +217,17 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         ex_e = __ldcg(A.eta_max + gown);
     }
     __syncthreads();
-    const int cidx = (ty + 2) * LX + (tx + 2);
+    if (use_tma) {  // every thread sees the box land (bounded wait)
+        const bool ok = mbar_wait(&sBar, 0);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                A.scal[SC_ERR] = 1.0;
+                mbar_wait(&sBar, 0);
+            }
+            return;
+        }
+    }
+    const int cidx = (ty + 2) * LX + (tx + HX);
     float vc[5];
 #pragma unroll
     for (int f = 0; f < 5; f++) vc[f] = sV[f * PS + cidx];
@@ -203,7 +237,9 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     }
 
     // ---- phase 2: depth, velocity, concentration per cell
-    for (int idx = tid; idx < PS; idx += NT) {
+    for (int k = tid; k < PSC; k += NT) {
+        const int ly = k / LXC;
+        const int idx = ly * LX + (k - ly * LXC) + (HX - 2);
         const float zz = sV[idx], HH = sV[PS + idx];
         const float hs = zz + (P.eta0f + HH);  // FP32 when clearly wet, FP64 near dryness
         const float h = (hs > kWetMarginf) ? hs : (float)depth64(zz, HH, eta0);
@@ -224,7 +260,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         float *dst;
         if (item < NXI) {
             int r = item / FXW, cx = item - r * FXW;
-            c = (r + 2) * LX + (cx + 1);
+            c = (r + 2) * LX + (cx + HX - 1);
             step = 1;
             dst = sFx + r * FXW + cx;
             fstride = TY * FXW;
@@ -234,7 +270,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         } else {
             int it = item - NXI;
             int ry = it / TX, cc = it - ry * TX;
-            c = (ry + 1) * LX + (cc + 2);
+            c = (ry + 1) * LX + (cc + HX);
             step = LX;
             dst = sFy + ry * TX + cc;
             fstride = FYH * TX;
@@ -278,7 +314,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
                 const int r = item / (TX + 1), e = item - r * (TX + 1);
                 a = get_face(sFx + (6 * TY + r) * FXW + e, TY * FXW);
                 b = get_face(sFx + r * FXW + (e + 1), TY * FXW);
-                fixed = (int)sM[(r + 2) * LX + e + 1] * (int)sM[(r + 2) * LX + e + 2];
+                fixed = (int)sM[(r + 2) * LX + e + HX - 1] * (int)sM[(r + 2) * LX + e + HX];
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
                 if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             } else {
@@ -286,7 +322,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
                 const int e = it / TX, c = it - e * TX;
                 a = get_face(sFy + (6 * FYH + e) * TX + c, FYH * TX);
                 b = get_face(sFy + (e + 1) * TX + c, FYH * TX);
-                fixed = (int)sM[(e + 1) * LX + c + 2] * (int)sM[(e + 2) * LX + c + 2];
+                fixed = (int)sM[(e + 1) * LX + c + HX] * (int)sM[(e + 2) * LX + c + HX];
                 if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
                 if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
             }
@@ -300,7 +336,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             if (periodic && (ex == 0 || ex == npx)) {
                 a = get_face(Rf, TY * FXW);
                 b = get_face(Lf, TY * FXW);
-                fixed = sM[ly * LX + e + 1];
+                fixed = sM[ly * LX + e + HX - 1];
                 seam = true;
                 seg = npx + ey;
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
@@ -308,20 +344,20 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             } else if (ex == 0) {
                 a = get_face(Lf, TY * FXW);
                 sgnn = -1;
-                fixed = sM[ly * LX + e + 2];
+                fixed = sM[ly * LX + e + HX];
                 bnd = true;
                 seg = 2 * npx + npy + ey;
                 outM = sFlux + 0 * 5 * FS + r * TX + e;
             } else if (ex == npx) {
                 a = get_face(Rf, TY * FXW);
-                fixed = sM[ly * LX + e + 1];
+                fixed = sM[ly * LX + e + HX - 1];
                 bnd = true;
                 seg = npx + ey;
                 outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
             } else {
                 a = get_face(Rf, TY * FXW);
                 b = get_face(Lf, TY * FXW);
-                fixed = (int)sM[ly * LX + e + 1] * (int)sM[ly * LX + e + 2];
+                fixed = (int)sM[ly * LX + e + HX - 1] * (int)sM[ly * LX + e + HX];
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
                 if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             }
@@ -335,7 +371,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             if (periodic && (ey == 0 || ey == npy)) {
                 a = get_face(Uf, FYH * TX);
                 b = get_face(Df, FYH * TX);
-                fixed = sM[(e + 1) * LX + c + 2];
+                fixed = sM[(e + 1) * LX + c + HX];
                 seam = true;
                 seg = npx + npy + ex;
                 if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
@@ -343,20 +379,20 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             } else if (ey == 0) {
                 a = get_face(Df, FYH * TX);
                 sgnn = -1;
-                fixed = sM[(e + 2) * LX + c + 2];
+                fixed = sM[(e + 2) * LX + c + HX];
                 bnd = true;
                 seg = ex;
                 outM = sFlux + 2 * 5 * FS + e * TX + c;
             } else if (ey == npy) {
                 a = get_face(Uf, FYH * TX);
-                fixed = sM[(e + 1) * LX + c + 2];
+                fixed = sM[(e + 1) * LX + c + HX];
                 bnd = true;
                 seg = npx + npy + ex;
                 outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
             } else {
                 a = get_face(Uf, FYH * TX);
                 b = get_face(Df, FYH * TX);
-                fixed = (int)sM[(e + 1) * LX + c + 2] * (int)sM[(e + 2) * LX + c + 2];
+                fixed = (int)sM[(e + 1) * LX + c + HX] * (int)sM[(e + 2) * LX + c + HX];
                 if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
                 if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
             }
@@ -576,10 +612,11 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
 
 // ---- single grid: one CTA per tile
 template <int TX, int TY, int MINB, int ORDER, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(TX *TY, MINB) stage32_kernel(Stage32Args A) {
+__global__ void __launch_bounds__(TX *TY, MINB)
+    stage32_kernel(const __grid_constant__ Stage32Args A, const __grid_constant__ Tma32 M) {
     extern __shared__ __align__(16) float smem32[];
-    stage32_tile<TX, TY, ORDER, FIRST, LAST>(A, A.phys, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x,
-                                             gridDim.x * gridDim.y, smem32);
+    stage32_tile<TX, TY, ORDER, FIRST, LAST>(A, A.phys, &M, blockIdx.x, blockIdx.y,
+                                             blockIdx.y * gridDim.x + blockIdx.x, gridDim.x * gridDim.y, smem32);
 }
 
 // ---- ensemble: persistent CTAs walking the tile list of all members
@@ -618,7 +655,7 @@ __global__ void __launch_bounds__(TX *TY, MINB) ens32_kernel(EnsArgs E, Phys32 c
         P.npy = sG.phys.npy;
         P.wbc = sG.phys.wbc;
         P.read_files = sG.phys.read_files;
-        stage32_tile<TX, TY, ORDER, FIRST, LAST>(sG, P, lt % ntx, lt / ntx, lt, E.members[m].ntiles, smem32);
+        stage32_tile<TX, TY, ORDER, FIRST, LAST>(sG, P, nullptr, lt % ntx, lt / ntx, lt, E.members[m].ntiles, smem32);
         __syncthreads();
         if (E.dynamic) {
             if (threadIdx.x == 0) sTile = atomicAdd(E.work, 1u);
@@ -728,7 +765,7 @@ namespace {
 struct Variant32 {
     int tx, ty, minb;
     size_t smem;
-    void (*k[3])(Stage32Args);
+    void (*k[3])(Stage32Args, Tma32);
     void (*e[3])(EnsArgs, Phys32);
 };
 
@@ -775,6 +812,27 @@ int single_variant() {
 int which(int order, int stage) { return (order == 2) ? (stage == 0 ? 0 : 1) : 2; }
 
 }  // namespace
+
+bool stage32_tma_maps(const float *bufA, const float *bufB, long long pitch, long long plane, int npx, int npy,
+                      CUtensorMap *tmA, CUtensorMap *tmB) {
+    EncodeTiledFn f = tensor_map_encoder();
+    const Variant32 &v = variants32(nullptr)[single_variant()];
+    const int lx = v.tx + 8, ly = v.ty + 4;  // T32<TX, TY>::LX, LY
+    if (!f || npx < lx || npy < ly) return false;
+    if (reinterpret_cast<uintptr_t>(bufA) % 16 || reinterpret_cast<uintptr_t>(bufB) % 16) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)npx, (cuuint64_t)npy, 5};
+    const cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(float), (cuuint64_t)plane * sizeof(float)};
+    const cuuint32_t box[3] = {(cuuint32_t)lx, (cuuint32_t)ly, 5};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const float *bufs[2] = {bufA, bufB};
+    CUtensorMap *maps[2] = {tmA, tmB};
+    for (int k = 0; k < 2; k++)
+        if (f(maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(bufs[k]), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    return true;
+}
 
 bool phys32_shared(const Phys32 &a, const Phys32 &b) {
     Phys32 x = a, y = b;
@@ -823,10 +881,10 @@ dim3 stage32_grid(int npx, int npy) {
     return dim3((npx + v.tx - 1) / v.tx, (npy + v.ty - 1) / v.ty);
 }
 
-cudaError_t stage32_launch(int order, int stage, const Stage32Args &a, cudaStream_t st) {
+cudaError_t stage32_launch(int order, int stage, const Stage32Args &a, const Tma32 &tm, cudaStream_t st) {
     const Variant32 &v = variants32(nullptr)[single_variant()];
     dim3 g = stage32_grid(a.phys.npx, a.phys.npy);
-    v.k[which(order, stage)]<<<g, v.tx * v.ty, v.smem, st>>>(a);
+    v.k[which(order, stage)]<<<g, v.tx * v.ty, v.smem, st>>>(a, tm);
     return cudaGetLastError();
 }
 

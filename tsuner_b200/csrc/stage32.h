@@ -1,6 +1,7 @@
 // stage32.h -- launch interface of the FP32 precision-form kernels (single
 // grid and batched ensemble).
 #pragma once
+#include <cuda.h>  // CUtensorMap
 #include <cuda_runtime.h>
 
 #include "physics32.cuh"
@@ -32,6 +33,13 @@ struct EnsMember {
     int ntx;          // tiles per row
 };
 
+// TMA descriptors of a single grid's two FP32 state buffers as 3-D tensors
+// [5][npy][npx] (boxes = the loaded tile); `on` = 0 means ordinary loads.
+struct Tma32 {
+    CUtensorMap a, b;
+    int on;
+};
+
 struct EnsArgs {
     const EnsMember *members;
     const int *tile_member;  // global tile -> member
@@ -43,7 +51,9 @@ struct EnsArgs {
 size_t stage32_smem_bytes();
 cudaError_t stage32_prepare();
 dim3 stage32_grid(int npx, int npy);
-cudaError_t stage32_launch(int order, int stage, const Stage32Args &a, cudaStream_t st);
+cudaError_t stage32_launch(int order, int stage, const Stage32Args &a, const Tma32 &tm, cudaStream_t st);
+bool stage32_tma_maps(const float *bufA, const float *bufB, long long pitch, long long plane, int npx, int npy,
+                      CUtensorMap *tmA, CUtensorMap *tmB);
 // tile-shape variants available to the ensemble kernel
 int stage32_num_tiles();
 void stage32_tile_shape(int variant, int *tx, int *ty, int *minb);

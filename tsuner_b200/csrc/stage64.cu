@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
     using T = Tile<TX, TY, NTHR>;
     constexpr int NT = T::NT, LX = T::LX, LY = T::LY, PS = T::PS, FXW = T::FXW, FYH = T::FYH;
     extern __shared__ __align__(16) double smem_raw[];
-    double *smem = reinterpret_cast<double *>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    double *smem = smem_align<128>(smem_raw);
     __shared__ uint64_t sBar;  // the tile's TMA load
     const Phys64 &P = A.phys;
     double *sV = smem;                  // [5][LY][LX]
