@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -39,6 +40,7 @@ struct TsuEnsemble {
     // device tables for the current tile shape
     std::vector<EnsMember> h_members;  // last uploaded member descriptors
     EnsMember *d_members = nullptr;
+    Tma32 *d_tmas = nullptr;  // per member TMA descriptors for the current tile shape
     int *d_tile_member = nullptr;
     unsigned *d_work = nullptr;
     unsigned ntiles = 0;
@@ -109,14 +111,28 @@ int build_tables(TsuEnsemble *E, int variant) {
         tile0 += M.ntiles;
         tm.insert(tm.end(), M.ntiles, i);
     }
+    // TMA descriptors of every member's state buffers for this tile shape
+    // (a member whose grid is too small for the box loads without TMA)
+    std::vector<Tma32> tmas(E->n);
+    const char *tma_env = std::getenv("TSU_STAGE_TMA");
+    const bool tma_allowed = !(tma_env && tma_env[0] == '0');
+    for (int i = 0; i < E->n; i++) {
+        TsuSolver *s = E->m[i];
+        tmas[i].on = tma_allowed && stage32_tma_maps(variant, (const float *)s->A, (const float *)s->B, s->pitch,
+                                                     s->plane, s->p.npx, s->p.npy, &tmas[i].a, &tmas[i].b);
+    }
     cudaFree(E->d_members);
     cudaFree(E->d_tile_member);
+    cudaFree(E->d_tmas);
     E->d_members = nullptr;
     E->d_tile_member = nullptr;
+    E->d_tmas = nullptr;
     ECK(cudaMalloc((void **)&E->d_members, sizeof(EnsMember) * E->n));
     ECK(cudaMalloc((void **)&E->d_tile_member, sizeof(int) * tm.size()));
+    ECK(cudaMalloc((void **)&E->d_tmas, sizeof(Tma32) * E->n));
     ECK(cudaMemcpy(E->d_members, mem.data(), sizeof(EnsMember) * E->n, cudaMemcpyHostToDevice));
     ECK(cudaMemcpy(E->d_tile_member, tm.data(), sizeof(int) * tm.size(), cudaMemcpyHostToDevice));
+    ECK(cudaMemcpy(E->d_tmas, tmas.data(), sizeof(Tma32) * E->n, cudaMemcpyHostToDevice));
     E->h_members.swap(mem);
     E->ntiles = tile0;
     E->variant = variant;
@@ -157,6 +173,7 @@ EnsArgs ens_args(const TsuEnsemble *E) {
     a.ntiles = E->ntiles;
     a.dynamic = E->dynamic;
     a.work = E->d_work;
+    a.tmas = E->d_tmas;
     return a;
 }
 
@@ -228,6 +245,7 @@ extern "C" int tsu_ens_destroy(TsuEnsemble *E) {
     drop_graph(E);
     cudaFree(E->d_members);
     cudaFree(E->d_tile_member);
+    cudaFree(E->d_tmas);
     cudaFree(E->d_work);
     if (E->e0) cudaEventDestroy(E->e0);
     if (E->e1) cudaEventDestroy(E->e1);

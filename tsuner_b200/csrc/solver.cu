@@ -226,7 +226,7 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
     const char *tma_env = std::getenv("TSU_STAGE_TMA");
     const bool tma_allowed = !(tma_env && tma_env[0] == '0');
     if (e == cudaSuccess && tma_allowed)
-        s->tma = s->fp32 ? stage32_tma_maps((const float *)s->A, (const float *)s->B, s->pitch, s->plane, p->npx,
+        s->tma = s->fp32 ? stage32_tma_maps(-1, (const float *)s->A, (const float *)s->B, s->pitch, s->plane, p->npx,
                                             p->npy, &s->tmA, &s->tmB)
                          : stage64_tma_maps((const double *)s->A, (const double *)s->B, s->pitch, s->plane, p->npx,
                                             p->npy, &s->tmA, &s->tmB);

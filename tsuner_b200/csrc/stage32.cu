@@ -655,7 +655,8 @@ __global__ void __launch_bounds__(TX *TY, MINB) ens32_kernel(EnsArgs E, Phys32 c
         P.npy = sG.phys.npy;
         P.wbc = sG.phys.wbc;
         P.read_files = sG.phys.read_files;
-        stage32_tile<TX, TY, ORDER, FIRST, LAST>(sG, P, nullptr, lt % ntx, lt / ntx, lt, E.members[m].ntiles, smem32);
+        stage32_tile<TX, TY, ORDER, FIRST, LAST>(sG, P, E.tmas ? E.tmas + m : nullptr, lt % ntx, lt / ntx, lt,
+                                                 E.members[m].ntiles, smem32);
         __syncthreads();
         if (E.dynamic) {
             if (threadIdx.x == 0) sTile = atomicAdd(E.work, 1u);
@@ -813,10 +814,14 @@ int which(int order, int stage) { return (order == 2) ? (stage == 0 ? 0 : 1) : 2
 
 }  // namespace
 
-bool stage32_tma_maps(const float *bufA, const float *bufB, long long pitch, long long plane, int npx, int npy,
-                      CUtensorMap *tmA, CUtensorMap *tmB) {
+bool stage32_tma_maps(int variant, const float *bufA, const float *bufB, long long pitch, long long plane, int npx,
+                      int npy, CUtensorMap *tmA, CUtensorMap *tmB) {
     EncodeTiledFn f = tensor_map_encoder();
-    const Variant32 &v = variants32(nullptr)[single_variant()];
+    int nv;
+    variants32(&nv);
+    if (variant < 0) variant = single_variant();
+    if (variant >= nv) return false;
+    const Variant32 &v = variants32(nullptr)[variant];
     const int lx = v.tx + 8, ly = v.ty + 4;  // T32<TX, TY>::LX, LY
     if (!f || npx < lx || npy < ly) return false;
     if (reinterpret_cast<uintptr_t>(bufA) % 16 || reinterpret_cast<uintptr_t>(bufB) % 16) return false;

@@ -46,14 +46,19 @@ struct EnsArgs {
     unsigned ntiles;
     int dynamic;     // 0: static stride over the tile list, 1: work counter
     unsigned *work;  // work counter (dynamic schedule)
+    // per member: TMA descriptors for the current tile shape, in device
+    // memory (written before the launch), or null
+    const Tma32 *tmas;
 };
 
 size_t stage32_smem_bytes();
 cudaError_t stage32_prepare();
 dim3 stage32_grid(int npx, int npy);
 cudaError_t stage32_launch(int order, int stage, const Stage32Args &a, const Tma32 &tm, cudaStream_t st);
-bool stage32_tma_maps(const float *bufA, const float *bufB, long long pitch, long long plane, int npx, int npy,
-                      CUtensorMap *tmA, CUtensorMap *tmB);
+// TMA descriptors of two FP32 state buffers with the boxes of tile variant
+// `variant` (-1: the single-grid variant); false if they cannot be made
+bool stage32_tma_maps(int variant, const float *bufA, const float *bufB, long long pitch, long long plane, int npx,
+                      int npy, CUtensorMap *tmA, CUtensorMap *tmB);
 // tile-shape variants available to the ensemble kernel
 int stage32_num_tiles();
 void stage32_tile_shape(int variant, int *tx, int *ty, int *minb);
