@@ -285,6 +285,26 @@ const char *tsu_corr_last_error(void);
  * overlap on the GPU race and must be serialised by the caller. */
 int tsu_cfl_dt_noalloc(const double *d_h, const double *d_qx, const double *d_qy, long pitch_elems,
                        const SimParams *p, double *d_dt, void *stream);
+/* Bulk host <-> device copies through the library's pinned staging chunks
+ * and host worker pool, the path every tsu_set_* / tsu_get_* call of this
+ * library uses (the reference copies with plain pageable cudaMemcpy,
+ * GPU/main_TSUNER.cu:113-122, :159-162, :199-207).  `nplanes` planes of
+ * `rows` rows x `width` bytes; host plane k at host[k] with row pitch
+ * `hpitch` bytes, device plane k at dev[k] with row pitch `dpitch` bytes;
+ * `device` is the CUDA ordinal that owns the device planes.  Host buffers
+ * may be pageable (staged through pinned chunks while host threads fill or
+ * drain them) or pinned (copied directly).  Ordered after earlier work on
+ * the legacy default stream; synchronous (they return once the bytes have
+ * arrived).  TSU_ERR_INVALID for NULL planes or width > pitch. */
+int tsu_copy_planes_to_device(int device, int nplanes, void *const *dev, size_t dpitch, const void *const *host,
+                              size_t hpitch, size_t width, size_t rows);
+int tsu_copy_planes_to_host(int device, int nplanes, void *const *host, size_t hpitch, const void *const *dev,
+                            size_t dpitch, size_t width, size_t rows);
+int tsu_copy_bytes_to_device(int device, void *dev, const void *host, size_t bytes);
+int tsu_copy_bytes_to_host(int device, void *host, const void *dev, size_t bytes);
+/* Host worker threads of the copy pool (TSU_HOST_THREADS, default
+ * min(cores, 16)); host only, no device use. */
+int tsu_host_threads(void);
 const char *tsu_strerror(int code);
 /* Detail text of the last failing call on this thread ("" if none). */
 const char *tsu_last_error(void);

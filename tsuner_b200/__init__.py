@@ -29,7 +29,8 @@ EXPORTS = [
     "tsu_create", "tsu_destroy", "tsu_set_state", "tsu_set_mask", "tsu_set_boundary_series",
     "tsu_reset", "tsu_step", "tsu_run_until", "tsu_sync", "tsu_get_state", "tsu_get_extrema",
     "tsu_get_time", "tsu_get_sums", "tsu_get_consts", "tsu_last_step_ms", "tsu_last_step_launches",
-    "tsu_state_device", "tsu_cfl_dt_noalloc", "tsu_strerror", "tsu_last_error", "tsu_version", "tsu_struct_sizes",
+    "tsu_state_device", "tsu_cfl_dt_noalloc", "tsu_copy_planes_to_device", "tsu_copy_planes_to_host",
+    "tsu_copy_bytes_to_device", "tsu_copy_bytes_to_host", "tsu_host_threads", "tsu_strerror", "tsu_last_error", "tsu_version", "tsu_struct_sizes",
     "tsu_ens_create", "tsu_ens_destroy", "tsu_ens_member", "tsu_ens_reset", "tsu_ens_step", "tsu_ens_sync",
     "tsu_ens_autotune", "tsu_ens_set_config", "tsu_ens_get_config", "tsu_ens_last_step_ms",
     "tsu_ens_last_step_launches", "tsu_ens_run_until",
@@ -115,6 +116,13 @@ def lib():
             "tsu_state_device": ([vp, C.POINTER(vp), C.POINTER(C.c_long), C.POINTER(C.c_long),
                                   C.POINTER(C.c_int)], C.c_int),
             "tsu_cfl_dt_noalloc": ([vp, vp, vp, C.c_long, C.POINTER(SimParams), vp, vp], C.c_int),
+            "tsu_copy_planes_to_device": ([C.c_int, C.c_int, C.POINTER(vp), C.c_size_t, C.POINTER(vp), C.c_size_t,
+                                           C.c_size_t, C.c_size_t], C.c_int),
+            "tsu_copy_planes_to_host": ([C.c_int, C.c_int, C.POINTER(vp), C.c_size_t, C.POINTER(vp), C.c_size_t,
+                                         C.c_size_t, C.c_size_t], C.c_int),
+            "tsu_copy_bytes_to_device": ([C.c_int, vp, vp, C.c_size_t], C.c_int),
+            "tsu_copy_bytes_to_host": ([C.c_int, vp, vp, C.c_size_t], C.c_int),
+            "tsu_host_threads": ([], C.c_int),
             "tsu_strerror": ([C.c_int], C.c_char_p),
             "tsu_last_error": ([], C.c_char_p),
             "tsu_version": ([], C.c_char_p),

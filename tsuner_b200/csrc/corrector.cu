@@ -50,6 +50,7 @@
 #include <new>
 #include <vector>
 
+#include "hostio.h"
 #include "async.cuh"
 #include "tsuner_b200.h"
 
@@ -866,9 +867,9 @@ extern "C" int tsu_corr_add_samples(TsuCorrector *c, int n, const float *coarse,
         c->fine = nf;
         c->cap = ncap;
     }
-    CCK(cudaMemcpyAsync(c->coarse + c->nsamples * cs, coarse, n * cs * 4, cudaMemcpyHostToDevice, c->st));
+    CCK(tsu::bytes_h2d(c->coarse + c->nsamples * cs, coarse, n * cs * 4, c->st));
     if (fine)
-        CCK(cudaMemcpyAsync(c->fine + c->nsamples * fs, fine, n * fs * 4, cudaMemcpyHostToDevice, c->st));
+        CCK(tsu::bytes_h2d(c->fine + c->nsamples * fs, fine, n * fs * 4, c->st));
     else
         CCK(cudaMemsetAsync(c->fine + c->nsamples * fs, 0, n * fs * 4, c->st));
     CCK(cudaStreamSynchronize(c->st));
@@ -987,9 +988,10 @@ extern "C" int tsu_corr_predict(TsuCorrector *c, int first, int n, float *out_hm
         if (!rc) rc = forward(c, 1);
         if (rc) break;
         apply_kernel<<<2 * num_sms(), 256, 0, c->st>>>(c->Yout, c->base, (long long)np, d_out, d_out + np);
+        void *outs[2] = {out_hmax + k * np, out_db + k * np};
+        const void *ins[2] = {d_out, d_out + np};
         if (cudaGetLastError() != cudaSuccess ||
-            cudaMemcpyAsync(out_hmax + k * np, d_out, np * 4, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
-            cudaMemcpyAsync(out_db + k * np, d_out + np, np * 4, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+            tsu::planes_d2h(2, outs, (size_t)c->W * 4, ins, (size_t)c->W * 4, (size_t)c->W * 4, c->H, c->st) != cudaSuccess ||
             cudaMemcpyAsync(bb.data(), c->base, 2 * np * 4, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
             cudaStreamSynchronize(c->st) != cudaSuccess) {
             snprintf(g_corr_msg, sizeof(g_corr_msg), "tsu_corr_predict: CUDA error");

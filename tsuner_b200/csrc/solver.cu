@@ -12,6 +12,7 @@
 // ~796 B per cell (GPU/main_TSUNER.cu:57-91).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -20,6 +21,7 @@
 #include <new>
 #include <vector>
 
+#include "hostio.h"
 #include "solver.h"
 #include "stage32.h"
 #include "stage64.h"
@@ -264,15 +266,19 @@ extern "C" int tsu_set_state(TsuSolver *s, const double *h, const double *qx, co
     if (r) return r;
     double *base = s->fp32 ? s->stage64 : (double *)s->A;
     const double *src[5] = {h, qx, qy, H, hc};
+    void *dst[5];
+    const void *from[5];
+    int n = 0;
     for (int f = 0; f < 5; f++) {
-        double *dst = base + f * s->plane;
         if (src[f]) {
-            CK(cudaMemcpy2DAsync(dst, s->pitch * sizeof(double), src[f], s->p.npx * sizeof(double),
-                                 s->p.npx * sizeof(double), s->p.npy, cudaMemcpyHostToDevice, s->st));
+            dst[n] = base + f * s->plane;
+            from[n++] = src[f];
         } else {
-            CK(cudaMemsetAsync(dst, 0, (size_t)s->plane * sizeof(double), s->st));
+            CK(cudaMemsetAsync(base + f * s->plane, 0, (size_t)s->plane * sizeof(double), s->st));
         }
     }
+    CK(tsu::planes_h2d(n, dst, s->pitch * sizeof(double), from, s->p.npx * sizeof(double), s->p.npx * sizeof(double),
+                       s->p.npy, s->st));
     if (s->fp32)
         CK(to32_launch(s->stage64, s->pitch, s->plane, s->p.npx, s->p.npy, s->sw.eta0, (float *)s->A, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -289,22 +295,31 @@ extern "C" int tsu_set_mask(TsuSolver *s, const int *fixH) {
         CK(cudaStreamSynchronize(s->st));
         return TSU_OK;
     }
-    const long long n = (long long)s->p.npx * s->p.npy;
-    std::vector<unsigned char> m;
-    try {
-        m.resize((size_t)n);
-    } catch (...) {
-        return TSU_ERR_HOST_OOM;
-    }
-    for (long long i = 0; i < n; i++) {
-        if (fixH[i] != 0 && fixH[i] != 1) {
-            snprintf(g_err, sizeof(g_err), "mask value %d at %lld is not 0 or 1", fixH[i], i);
+    const size_t npx = s->p.npx, npy = s->p.npy;
+    // Validate first (the mask is left as it was on a bad value), in parallel
+    // row ranges; the first bad index is the first one of the lowest range.
+    const int parts = (int)std::min<size_t>(npy, 4 * (size_t)tsu::host_threads());
+    std::vector<long long> bad(parts, -1);
+    tsu::host_parallel(parts, [&](int q) {
+        const size_t a = npy * q / parts * npx, b = npy * (q + 1) / parts * npx;
+        for (size_t i = a; i < b; i++)
+            if (fixH[i] != 0 && fixH[i] != 1) {
+                bad[q] = (long long)i;
+                return;
+            }
+    });
+    for (int q = 0; q < parts; q++)
+        if (bad[q] >= 0) {
+            snprintf(g_err, sizeof(g_err), "mask value %d at %lld is not 0 or 1", fixH[bad[q]], bad[q]);
             return TSU_ERR_INVALID;
         }
-        m[(size_t)i] = (unsigned char)fixH[i];
-    }
-    CK(cudaMemcpy2DAsync(s->mask, s->pitch, m.data(), s->p.npx, s->p.npx, s->p.npy, cudaMemcpyHostToDevice, s->st));
-    CK(cudaStreamSynchronize(s->st));
+    void *dst[1] = {s->mask};
+    const void *from[1] = {fixH};
+    CK(tsu::planes_h2d(1, dst, s->pitch, from, npx * sizeof(int), npx, npy, s->st,
+                       [&](int, size_t r0, size_t nr, unsigned char *out) {
+                           const int *in = fixH + r0 * npx;
+                           for (size_t i = 0; i < nr * npx; i++) out[i] = (unsigned char)in[i];
+                       }));
     return TSU_OK;
 }
 
@@ -323,9 +338,8 @@ extern "C" int tsu_set_boundary_series(TsuSolver *s, const double *CC, const dou
     size_t n = (size_t)(2 * s->p.npx + 2 * s->p.npy) * 4 * timeCC;
     CK(cudaMalloc((void **)&s->CC, n * sizeof(double)));
     CK(cudaMalloc((void **)&s->tCC, timeCC * sizeof(double)));
-    CK(cudaMemcpyAsync(s->CC, CC, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
-    CK(cudaMemcpyAsync(s->tCC, tCC, timeCC * sizeof(double), cudaMemcpyHostToDevice, s->st));
-    CK(cudaStreamSynchronize(s->st));
+    CK(tsu::bytes_h2d(s->CC, CC, n * sizeof(double), s->st));
+    CK(tsu::bytes_h2d(s->tCC, tCC, timeCC * sizeof(double), s->st));
     s->timeCC = timeCC;
     s->invalidate_graph();
     return TSU_OK;
@@ -522,13 +536,17 @@ extern "C" int tsu_get_state(TsuSolver *s, double *V) {
         if (r) return r;
         CK(to64_launch((const float *)s->current(), s->pitch, s->plane, s->p.npx, s->p.npy, s->sw.eta0, s->stage64,
                        s->st));
-        CK(cudaStreamSynchronize(s->st));
         cur = s->stage64;
     }
     const size_t n = (size_t)s->p.npx * s->p.npy;
-    for (int f = 0; f < 5; f++)
-        CK(cudaMemcpy2D(V + f * n, s->p.npx * sizeof(double), cur + f * s->plane, s->pitch * sizeof(double),
-                        s->p.npx * sizeof(double), s->p.npy, cudaMemcpyDeviceToHost));
+    void *dst[5];
+    const void *from[5];
+    for (int f = 0; f < 5; f++) {
+        dst[f] = V + f * n;
+        from[f] = cur + f * s->plane;
+    }
+    CK(tsu::planes_d2h(5, dst, s->p.npx * sizeof(double), from, s->pitch * sizeof(double), s->p.npx * sizeof(double),
+                       s->p.npy, s->st));
     return TSU_OK;
 }
 
@@ -537,20 +555,26 @@ extern "C" int tsu_get_extrema(TsuSolver *s, double *hmax, double *bmin, double 
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->st));
     void *src[3] = {s->hmax, s->bmin, s->eta};
-    double *dst[3] = {hmax, bmin, eta_max};
-    for (int f = 0; f < 3; f++) {
-        if (!dst[f]) continue;
-        const double *from = (const double *)src[f];
-        if (s->fp32) {
-            int r = staging(s);
-            if (r) return r;
-            CK(widen_launch((const float *)src[f], s->stage64, s->plane, s->st));
-            CK(cudaStreamSynchronize(s->st));
-            from = s->stage64;
-        }
-        CK(cudaMemcpy2D(dst[f], s->p.npx * sizeof(double), from, s->pitch * sizeof(double), s->p.npx * sizeof(double),
-                        s->p.npy, cudaMemcpyDeviceToHost));
+    double *want[3] = {hmax, bmin, eta_max};
+    void *dst[3];
+    const void *from[3];
+    int n = 0;
+    if (s->fp32) {
+        int r = staging(s);
+        if (r) return r;
     }
+    for (int f = 0; f < 3; f++) {
+        if (!want[f]) continue;
+        const double *d = (const double *)src[f];
+        if (s->fp32) {  // widen into the FP64 staging planes, one per field
+            CK(widen_launch((const float *)src[f], s->stage64 + f * s->plane, s->plane, s->st));
+            d = s->stage64 + f * s->plane;
+        }
+        dst[n] = want[f];
+        from[n++] = d;
+    }
+    CK(tsu::planes_d2h(n, dst, s->p.npx * sizeof(double), from, s->pitch * sizeof(double), s->p.npx * sizeof(double),
+                       s->p.npy, s->st));
     return TSU_OK;
 }
 
