@@ -253,30 +253,45 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     __syncthreads();
     const float hcell = sV[5 * PS + cidx];
 
-    // ---- phase 3: faces
-    constexpr int NXI = FXW * TY, NYI = TX * FYH;
-    for (int item = tid; item < NXI + NYI; item += NT) {
-        int c, step, fstride, side, didx = -1;
+    // ---- phase 3: faces.  A thread's items: the x faces of its own cell,
+    // its y faces, and (the first NFR threads) one fringe item: the x faces
+    // of halo column -1 or TX, or the y faces of halo row -1 or TY.  One
+    // call site of the reconstruction serves every item.
+    constexpr int NFRX = 2 * TY, NFR = 2 * TY + 2 * TX;
+    static_assert(NFR <= NT, "one fringe face item per thread at most");
+    const int nk3 = (tid < NFR) ? 3 : 2;
+#pragma unroll 1
+    for (int k = 0; k < nk3; k++) {
+        bool xdir;
+        int lx, ly;
+        if (k < 2) {
+            xdir = (k == 0);
+            lx = tx;
+            ly = ty;
+        } else if (tid < NFRX) {
+            xdir = true;
+            ly = tid >> 1;
+            lx = (tid & 1) ? TX : -1;
+        } else {
+            const int j = tid - NFRX;
+            xdir = false;
+            lx = j >> 1;
+            ly = (j & 1) ? TY : -1;
+        }
+        const int c = (ly + 2) * LX + (lx + HX);
+        const int step = xdir ? 1 : LX;
         float *dst;
-        if (item < NXI) {
-            int r = item / FXW, cx = item - r * FXW;
-            c = (r + 2) * LX + (cx + HX - 1);
-            step = 1;
-            dst = sFx + r * FXW + cx;
+        int fstride, side, didx = -1;
+        if (xdir) {
+            dst = sFx + ly * FXW + (lx + 1);
             fstride = TY * FXW;
             side = 6 * TY * FXW;
-            int tc = cx - 1;
-            if (tc >= 0 && tc < TX) didx = r * TX + tc;
+            if (k == 0) didx = ty * TX + tx;
         } else {
-            int it = item - NXI;
-            int ry = it / TX, cc = it - ry * TX;
-            c = (ry + 1) * LX + (cc + HX);
-            step = LX;
-            dst = sFy + ry * TX + cc;
+            dst = sFy + (ly + 1) * TX + lx;
             fstride = FYH * TX;
             side = 6 * FYH * TX;
-            int tr = ry - 1;
-            if (tr >= 0 && tr < TY) didx = TY * TX + tr * TX + cc;
+            if (k == 1) didx = TY * TX + ty * TX + tx;
         }
         Face32 fm, fp;
         if (ORDER == 2) {
@@ -300,26 +315,52 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     // ---- phase 4: edges.  One call site of the edge flux serves every kind
     // of edge, so the arithmetic (and its contraction into FMAs) of an edge
     // does not depend on which tile, tile shape or schedule computes it.
-    constexpr int NV = (TX + 1) * TY, NH = TX * (TY + 1);
     constexpr int FS = TY * TX;
     const bool series_on = !inner && P.read_files && (t < __ldg(A.tCC + (A.timeCC - 2)));
-    for (int item = tid; item < NV + NH; item += NT) {
+    // A thread's items: the vertical edge east of its own cell, the
+    // horizontal edge north of it, and (the first TX + TY threads) one fringe
+    // edge: the west edge of row `tid` or the south edge of column tid - TY.
+    constexpr int NFE = TX + TY;
+    static_assert(NFE <= NT, "one fringe edge per thread at most");
+    const int nk4 = (tid < NFE) ? 3 : 2;
+#pragma unroll 1
+    for (int k = 0; k < nk4; k++) {
         Face32 a, b;
         int sgnn = 1, fixed, seg = 0;
         bool bnd = false, seam = false;
-        const bool vert = item < NV;
+        // vertical edge e (0..TX) of row r, or horizontal edge e (0..TY) of column c
+        bool vert;
+        int r, e, c;
+        if (k == 0) {
+            vert = true;
+            r = ty;
+            e = tx + 1;
+            c = 0;
+        } else if (k == 1) {
+            vert = false;
+            r = 0;
+            e = ty + 1;
+            c = tx;
+        } else if (tid < TY) {
+            vert = true;
+            r = tid;
+            e = 0;
+            c = 0;
+        } else {
+            vert = false;
+            r = 0;
+            e = 0;
+            c = tid - TY;
+        }
         float *outM = nullptr, *outP = nullptr;
         if (inner) {  // interior edges only (uniform per tile): no bounds or boundary cases
             if (vert) {
-                const int r = item / (TX + 1), e = item - r * (TX + 1);
                 a = get_face(sFx + (6 * TY + r) * FXW + e, TY * FXW);
                 b = get_face(sFx + r * FXW + (e + 1), TY * FXW);
                 fixed = (int)sM[(r + 2) * LX + e + HX - 1] * (int)sM[(r + 2) * LX + e + HX];
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
                 if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             } else {
-                const int it = item - NV;
-                const int e = it / TX, c = it - e * TX;
                 a = get_face(sFy + (6 * FYH + e) * TX + c, FYH * TX);
                 b = get_face(sFy + (e + 1) * TX + c, FYH * TX);
                 fixed = (int)sM[(e + 1) * LX + c + HX] * (int)sM[(e + 2) * LX + c + HX];
@@ -327,7 +368,6 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
                 if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
             }
         } else if (vert) {
-            const int r = item / (TX + 1), e = item - r * (TX + 1);
             const int ex = x0 + e, ey = y0 + r;
             if (ey >= npy || ex > npx) continue;
             const int ly = r + 2;
@@ -362,8 +402,6 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
                 if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             }
         } else {
-            const int it = item - NV;
-            const int e = it / TX, c = it - e * TX;
             const int ex = x0 + c, ey = y0 + e;
             if (ex >= npx || ey > npy) continue;
             const float *Uf = sFy + (6 * FYH + e) * TX + c;
