@@ -826,17 +826,19 @@ Variant32 make_variant32() {
 
 // tile W x H / minimum resident CTAs per SM (register budget)
 const Variant32 *variants32(int *n) {
-    static Variant32 v[8] = {make_variant32<32, 8, 2>(),  make_variant32<16, 16, 2>(), make_variant32<32, 16, 1>(),
+    static Variant32 v[9] = {make_variant32<32, 8, 2>(),  make_variant32<16, 16, 2>(), make_variant32<32, 16, 1>(),
                              make_variant32<64, 4, 2>(),  make_variant32<32, 8, 3>(),  make_variant32<16, 16, 3>(),
-                             make_variant32<32, 8, 4>(),  make_variant32<32, 16, 2>()};
-    if (n) *n = 8;
+                             make_variant32<32, 8, 4>(),  make_variant32<32, 16, 2>(), make_variant32<16, 16, 4>()};
+    if (n) *n = 9;
     return v;
 }
 
-// single-grid variant: TSU_TILE32 = index into variants32; default 32x8
-// with 4 resident CTAs per SM (measured fastest: 32 warps per SM hide the
-// fixed-latency dependencies of the flux arithmetic; 16 warps did not)
-constexpr int kSingleDefault = 6;
+// single-grid variant: TSU_TILE32 = index into variants32; default 16x16
+// with 4 resident CTAs per SM (measured fastest at 4096^2: 32 warps per SM
+// hide the fixed-latency dependencies of the flux arithmetic, 16 warps did
+// not; 16x16 has a smaller face/edge fringe than 32x8, 7357 vs 7320
+// Mcell-steps/s)
+constexpr int kSingleDefault = 8;
 int single_variant() {
     static int k = [] {
         int n;
