@@ -678,7 +678,12 @@ __global__ void __launch_bounds__(TX *TY, MINB) ens32_kernel(EnsArgs E, Phys32 c
     }
     while (tile < E.ntiles) {
         const int m = E.tile_member[tile];
-        if (threadIdx.x == 0) sG = E.members[m].g;
+        // the member's descriptor, one 8-byte word per thread (a copy by one
+        // thread is a chain of dependent loads every tile waits for)
+        static_assert(sizeof(Stage32Args) % 8 == 0 && sizeof(Stage32Args) / 8 <= TX * TY, "descriptor copy");
+        if (threadIdx.x < sizeof(Stage32Args) / 8)
+            reinterpret_cast<unsigned long long *>(&sG)[threadIdx.x] =
+                __ldg(reinterpret_cast<const unsigned long long *>(&E.members[m].g) + threadIdx.x);
         __syncthreads();
         const unsigned lt = tile - E.members[m].tile0;
         const int ntx = E.members[m].ntx;
