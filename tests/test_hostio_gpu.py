@@ -151,3 +151,42 @@ def test_mask_bad_value_reported_at_its_index():
         s.set_mask(m)  # a valid mask is accepted afterwards
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_boundary_series_replaced_in_place(precision):
+    """The boundary series buffers are kept across tsu_set_boundary_series
+    calls and only grown.  A series replaced by a shorter one, and a short
+    one replaced by a longer one (with steps of the old series still queued
+    on the solver's stream), must step exactly like a fresh solver given only
+    the final series."""
+    dev()
+    from tsuner_b200 import workloads as W
+    w = W.nwave_shelf(npx=256, npy=192, steps=40)
+    H = w.V[3]
+    long_s = W.boundary_series(H, w.slr, 4000.0, amp=3.0, period=600.0)  # ~23 MB: staged upload
+    short_s = W.boundary_series(H, w.slr, 500.0, amp=2.0, period=300.0)
+    sw = make_switches(order=2, wbc=1, read_files=1, precision=precision, eta0=w.slr)
+
+    def run(series_list):
+        s = T.Solver(w.p, sw)
+        try:
+            for k, (CC, tCC) in enumerate(series_list):
+                s.set_state(w.V)
+                s.set_mask(w.mask)
+                s.set_boundary_series(CC, tCC)
+                s.reset()
+                s.step(5 if k + 1 < len(series_list) else 40)
+            return s.state(), s.time()
+        finally:
+            s.close()
+
+    for first, final in ((long_s, short_s), (short_s, long_s)):
+        V1, t1 = run([first, final])
+        V0, t0 = run([final])
+        assert np.array_equal(V1, V0)
+        assert t1 == t0
+    # the two series really give different runs
+    Va, _ = run([long_s])
+    Vb, _ = run([short_s])
+    assert not np.array_equal(Va, Vb)

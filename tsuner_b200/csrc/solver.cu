@@ -332,12 +332,30 @@ extern "C" int tsu_set_boundary_series(TsuSolver *s, const double *CC, const dou
     for (unsigned long q = 1; q < timeCC; q++)
         if (fabs((tCC[q] - tCC[0]) - q * dtc) > 1e-9 * fabs(dtc) * q) return TSU_ERR_INVALID;
     CK(cudaSetDevice(s->device));
-    cudaFree(s->CC);
-    cudaFree(s->tCC);
-    s->CC = s->tCC = nullptr;
+    // The buffers are kept and only grown: a free + allocate pair per call
+    // occasionally took hundreds of milliseconds.  The copies below are
+    // ordered on the solver's stream after any steps still in flight.  Until
+    // the new series has arrived the solver has none (a failed upload leaves
+    // it unable to step rather than holding half of a series).
+    s->timeCC = 0;
+    s->invalidate_graph();
     size_t n = (size_t)(2 * s->p.npx + 2 * s->p.npy) * 4 * timeCC;
-    CK(cudaMalloc((void **)&s->CC, n * sizeof(double)));
-    CK(cudaMalloc((void **)&s->tCC, timeCC * sizeof(double)));
+    if (n > s->CC_cap) {
+        CK(cudaStreamSynchronize(s->st));
+        cudaFree(s->CC);
+        s->CC = nullptr;
+        s->CC_cap = 0;
+        CK(cudaMalloc((void **)&s->CC, n * sizeof(double)));
+        s->CC_cap = n;
+    }
+    if (timeCC > s->tCC_cap) {
+        CK(cudaStreamSynchronize(s->st));
+        cudaFree(s->tCC);
+        s->tCC = nullptr;
+        s->tCC_cap = 0;
+        CK(cudaMalloc((void **)&s->tCC, timeCC * sizeof(double)));
+        s->tCC_cap = timeCC;
+    }
     CK(tsu::bytes_h2d(s->CC, CC, n * sizeof(double), s->st));
     CK(tsu::bytes_h2d(s->tCC, tCC, timeCC * sizeof(double), s->st));
     s->timeCC = timeCC;
@@ -441,6 +459,10 @@ int TsuSolver::launch_steps(long n) {
 
 extern "C" int tsu_step(TsuSolver *s, long nsteps) {
     if (!s || nsteps < 0) return TSU_ERR_INVALID;
+    if (s->sw.read_files && s->timeCC < 2) {  // e.g. the last series upload failed
+        snprintf(g_err, sizeof(g_err), "read_files is set but no boundary series is loaded");
+        return TSU_ERR_INVALID;
+    }
     if (!s->ready) {
         int r = tsu_reset(s);
         if (r) return r;
@@ -491,6 +513,10 @@ extern "C" int tsu_sync(TsuSolver *s) {
 
 extern "C" int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *steps_done) {
     if (!s || max_steps < 0) return TSU_ERR_INVALID;
+    if (s->sw.read_files && s->timeCC < 2) {  // e.g. the last series upload failed
+        snprintf(g_err, sizeof(g_err), "read_files is set but no boundary series is loaded");
+        return TSU_ERR_INVALID;
+    }
     if (!s->ready) {
         int r = tsu_reset(s);
         if (r) return r;

@@ -21,6 +21,7 @@ struct TsuSolver {
     double *stage64 = nullptr;  // FP32 form: FP64 staging planes for upload/download
     unsigned char *mask = nullptr;
     double *CC = nullptr, *tCC = nullptr;
+    size_t CC_cap = 0, tCC_cap = 0;  // allocated elements (kept across series)
     unsigned long timeCC = 0;
     double *scal = nullptr, *partials = nullptr;
     size_t npartials = 0;
