@@ -67,10 +67,14 @@ def test_conv_forward_fp32_out(shape):
     assert err <= 1e-4 * max(1.0, ref.abs().max().item()), err
 
 
-def test_conv_forward_relu_bf16_out_and_gate():
+@pytest.mark.parametrize("shape", [(2, 40, 24), (1, 37, 29), (3, 16, 8), (1, 130, 67)])
+def test_conv_forward_relu_bf16_out_and_gate(shape):
+    """BF16 output goes through the staged, row-coalesced epilogue; ragged
+    widths and heights leave partial tile rows and partial warps."""
     d = dev()
-    X, Wt, b = rand_case(2, 40, 24, 2)
-    G = bf16(torch.randn(2, 40, 24, 32)).to(d)
+    n, h, w = shape
+    X, Wt, b = rand_case(n, h, w, 2)
+    G = bf16(torch.randn(n, h, w, 32)).to(d)
     ref = torch.relu(F.conv2d(X.float().to(d), Wt.float().to(d), b.to(d), padding=1))
     ref = nhwc(ref) * (G.float() > 0)
     Y = conv(nhwc(X).to(d), wk_from_torch(Wt).to(d), b.to(d), relu=1, gate=G, out_fp32=False)
@@ -78,6 +82,17 @@ def test_conv_forward_relu_bf16_out_and_gate():
     err = (Y.float() - ref).abs()
     assert (err <= 2.0 ** -8 * ref.abs() + 1e-6).all(), err.max().item()
     assert bool(((ref == 0) == (Y.float() == 0)).all())
+
+
+@pytest.mark.parametrize("shape", [(1, 37, 29), (2, 64, 64)])
+def test_conv_forward_bf16_out_no_gate(shape):
+    d = dev()
+    n, h, w = shape
+    X, Wt, b = rand_case(n, h, w, 6)
+    ref = nhwc(F.conv2d(X.float().to(d), Wt.float().to(d), b.to(d), padding=1))
+    Y = conv(nhwc(X).to(d), wk_from_torch(Wt).to(d), b.to(d), relu=0, out_fp32=False)
+    err = (Y.float() - ref).abs()
+    assert (err <= 2.0 ** -8 * ref.abs() + 1e-6).all(), err.max().item()
 
 
 def test_conv_input_gradient_with_flipped_weights():
