@@ -28,13 +28,17 @@
 //
 // Weight gradient (conv3x3_wgrad_kernel): dW[cout][tap][cin] =
 //   sum_p dZ[p][cout] X[p + off(tap)][cin], a GEMM with the pixels as the
-// reduction dimension: D[288 (tap,cin) x 32 (cout)] in three M=128 blocks,
-// MN-major operands (8 pixels x 16 bytes per core matrix): A is copied from
-// the patch planes in 128-byte core matrices, B is the dZ tile itself (both
-// loaded by TMA).  Row 288 of A is all ones, so D[288][cout] is the bias
-// gradient.  Each CTA
-// accumulates a strip of tiles in TMEM and adds its partial result to the
-// FP32 gradients with atomics.
+// reduction dimension.  The input patch is loaded by one TMA box of a 5-D
+// view of the NHWC tensor that lands as [row][channel quarter][x][8
+// channels]: for a horizontal tap offset dx, the 12 core-matrix groups
+// (dy, quarter) of the shifted patch are then 160 B apart, so
+// D_dx[dy * 32 + cin][cout] is one M = 128 MMA per 16 pixels with A read in
+// place (rows 96..127 see the next patch row and are ignored) and B = the dZ
+// tile as loaded; no operand copy is made.  Three accumulators (dx = 0..2)
+// take 96 TMEM columns.  Two stages: the next tile loads while this one's
+// MMAs run.  The bias gradient is summed from the dZ tile on the CUDA cores.
+// Each CTA accumulates a strip of tiles in TMEM and adds its partial result
+// to the FP32 gradients with atomics.
 //
 // Every mbarrier wait is bounded (globaltimer); on expiry the kernel sets
 // the error word, waits once more (bounded) for its MMAs, frees its TMEM and
@@ -76,10 +80,15 @@ static_assert(kPlane % 128 == 0 && kPlane >= kPlaneData && kWBytes % 128 == 0, "
 // wgrad: patch + dZ tile + A for half of the 8 K steps (4 x 3 M blocks x 4 KB);
 // ~67 KB, so three CTAs fit on an SM
 constexpr int kZPlane = 128 * 16;
-constexpr int kABlock = 4096;
-constexpr int kWgHalf = 4;
-constexpr int kWgSmem = 1024 + kPatch + 4 * kZPlane + kWgHalf * 3 * kABlock + 64;
-constexpr int kWgCtasPerSm = 3;
+// weight gradient: the patch as [row][channel quarter][x][8 channels]
+constexpr int kRowQ = 4 * PW * 16;           // one patch row: 640 B
+constexpr int kWgPatch = PH * kRowQ;         // 11520 B
+constexpr int kWgPatchBuf = 12288;           // + the row read by the ignored A rows 96..127
+constexpr int kWgStage = kWgPatchBuf + 4 * kZPlane;
+constexpr int kWgSmem = 1024 + 2 * kWgStage + 64;
+constexpr int kWgCtasPerSm = 4;              // 128 TMEM columns each
+static_assert(kWgPatch + kRowQ <= kWgPatchBuf && kWgPatchBuf % 128 == 0 && kWgStage % 128 == 0, "wgrad buffers");
+static_assert(kWgCtasPerSm * (kWgSmem + 1024) <= 228 * 1024 && kWgCtasPerSm * 128 <= 512, "wgrad residency");
 
 __device__ int g_corr_err;  // set by a kernel whose wait expired
 
@@ -375,31 +384,19 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __gr
 
 // Weight (and bias) gradient, accumulated into dW[cout][288] and db[32].
 __global__ void __launch_bounds__(128, kWgCtasPerSm)
-    conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmZ, int nimg,
+    conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmXr, const __grid_constant__ CUtensorMap tmZ, int nimg,
                          int H, int W, float *__restrict__ dW, float *__restrict__ db) {
     extern __shared__ unsigned char sm_raw[];
-    unsigned char *sm = smem_align<1024>(sm_raw);
-    unsigned char *sP = sm;
-    unsigned char *sZ = sm + kPatch;
-    unsigned char *sA = sZ + 4 * kZPlane;
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(sA + kWgHalf * 3 * kABlock);  // MMA done
-    uint64_t *full = mbar + 1;                                                   // tile loaded
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
+    unsigned char *sm = smem_align<1024>(sm_raw);  // two stages: patch (12288 B) + dZ planes (4 x 2048 B)
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm + 2 * kWgStage);  // [2] stage loaded
+    uint64_t *done = full + 2;                                          // [2] MMAs of the stage finished
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(full + 4);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TileGeom G = tile_geom(nimg, H, W);
 
-    // rows 288..383 of A: zero, except row 288 = 1 (bias gradient); these
-    // core matrices (M groups 36..47 = block 2 groups 4..15) are never rewritten
-    for (int c = tid; c < kWgHalf * 12 * 2 * 8; c += 128) {  // (s, group, kgroup, 16-byte row)
-        const int r = c & 7, kg = (c >> 3) & 1, g = 4 + ((c >> 4) % 12), s = c / 192;
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (g == 4) v.x = 0x3F80u;  // bf16 1.0 in element 0: row 288 of this pixel
-        *reinterpret_cast<uint4 *>(sA + (s * 3 + 2) * kABlock + g * 256 + kg * 128 + r * 16) = v;
-    }
     if (warp == 0) tmem_alloc(tslot, 128);
     if (tid == 0) {
-        mbar_init(mbar, 1);
-        mbar_init(full, 1);
+        for (int k = 0; k < 4; k++) mbar_init(&full[k], 1);
         mbar_init_fence();
     }
     fence_before();
@@ -407,85 +404,126 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
     fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t id = idesc(128, 32, 1, 1);
-    const uint32_t a_u32 = smem_u32(sA), z_u32 = smem_u32(sZ);
+    const uint32_t sm_u32 = smem_u32(sm);
 
-    bool failed = false;
-    int i = 0, nwait = 0;
-    for (int t = blockIdx.x; t < G.total; t += gridDim.x, i++) {
+    // tile t -> stage st: the patch (one 5-D box, zero fill outside the
+    // image) and the dZ tile (four channel-quarter boxes)
+    auto issue = [&](int t, int st) {
         const int img = t / G.per_img, r = t - img * G.per_img;
         const int tyi = r / G.ntx, txi = r - tyi * G.ntx;
         const int x0 = txi * TXP, y0 = tyi * TYP;
-        if (tid == 0) {  // patch (4 x 2880 B) and the dZ tile (4 x 8 x 16 x 8 channels) by TMA
-            mbar_expect_tx(full, 4 * kPlaneData + 4 * kZPlane);
-            issue_patch(&tmX, img, x0, y0, sP, full);
+        unsigned char *stg = sm + st * kWgStage;
+        mbar_expect_tx(&full[st], kWgPatch + 4 * kZPlane);
+        tma_load_5d(stg, &tmXr, 0, x0 - 1, 0, y0 - 1, img, &full[st]);
 #pragma unroll
-            for (int q = 0; q < 4; q++) tma_load_4d(sZ + q * kZPlane, &tmZ, 8 * q, x0, y0, img, full);
-        }
-        const bool loaded = mbar_wait(full, i & 1);
-        if (__syncthreads_or(!loaded)) {
-            failed = true;
-            if (tid == 0) {
-                atomicExch(&g_corr_err, 1);
-                mbar_wait(full, i & 1);
+        for (int q = 0; q < 4; q++) tma_load_4d(stg + kWgPatchBuf + q * kZPlane, &tmZ, 8 * q, x0, y0, img, &full[st]);
+    };
+    int last_load = -1, last_mma = -1;  // iterations whose load / MMAs tid 0 issued (for the error path)
+    if (tid == 0 && (int)blockIdx.x < G.total) {
+        issue(blockIdx.x, 0);
+        last_load = 0;
+    }
+    float dbp[8];  // bias gradient partials: cout q * 8 + 2 * (lane & 3) + {0, 1}
+#pragma unroll
+    for (int k = 0; k < 8; k++) dbp[k] = 0.f;
+
+    bool failed = false;
+    int i = 0;
+    for (int t = blockIdx.x; t < G.total; t += gridDim.x, i++) {
+        const int b = i & 1;
+        // first the next tile into the other stage, once the MMAs of the tile
+        // it held have finished (its bias reads ended at the last barrier),
+        // so that two loads are in flight while this tile waits for its data
+        bool ok = true;
+        const int tn = t + gridDim.x;
+        if (tid == 0 && tn < G.total) {
+            if (i >= 1) ok = mbar_wait(&done[b ^ 1], ((i - 1) >> 1) & 1);
+            if (ok) {
+                issue(tn, b ^ 1);
+                last_load = i + 1;
             }
+        }
+        const bool loaded = mbar_wait(&full[b], (i >> 1) & 1);
+        if (__syncthreads_or(!loaded || !ok)) {
+            failed = true;
             break;
         }
-        // two rounds of 4 K steps (tile rows 0-7, then 8-15)
-        for (int hh = 0; hh < 2 && !failed; hh++) {
-            // A core matrices (s, G = tap*4 + quarter, kgroup): 8 pixels of
-            // tile row 2s + kg shifted by the tap, 8 channels each; 8 lanes
-            // copy one 128-byte core matrix (no bank conflicts)
-            for (int c = tid; c < kWgHalf * 36 * 2 * 8; c += 128) {
-                const int k = c & 7, blk = c >> 3;
-                const int sl = blk / 72, rem = blk - sl * 72, Gm = rem >> 1, kg = rem & 1;
-                const int tap = Gm >> 2, q = Gm & 3, dy = tap / 3, dx = tap - dy * 3;
-                const int py = 2 * (kWgHalf * hh + sl) + kg;
-                const uint4 *src = reinterpret_cast<const uint4 *>(sP + q * kPlane + ((py + dy) * PW + dx) * 16);
-                uint4 *dst =
-                    reinterpret_cast<uint4 *>(sA + (sl * 3 + (Gm >> 4)) * kABlock + (Gm & 15) * 256 + kg * 128);
-                dst[k] = src[k];
-            }
-            fence_async_smem();
-            fence_before();
-            __syncthreads();
-            fence_after();
-            if (tid == 0) {
+        if (tid == 0) {
+            // D[dy * 32 + cin (+ 32 ignored rows)][cout] for each dx: A = the
+            // shifted patch (M groups (dy, quarter) 160 B apart, K groups =
+            // tile rows 640 B apart), B = dZ (N groups = quarters, K groups =
+            // tile rows 128 B apart); 16 pixels (two tile rows) per MMA
+            const uint32_t pb = sm_u32 + b * kWgStage, zb = pb + kWgPatchBuf;
 #pragma unroll 1
-                for (int sl = 0; sl < kWgHalf; sl++) {
-                    const int s = kWgHalf * hh + sl;
-                    const uint64_t dbd = sdesc(z_u32 + s * 256, 128, kZPlane);
+            for (int s = 0; s < 8; s++) {
+                const uint64_t dz = sdesc(zb + s * 256, 128, kZPlane);
 #pragma unroll
-                    for (int b = 0; b < 3; b++) {
-                        const uint64_t da = sdesc(a_u32 + (sl * 3 + b) * kABlock, 128, 256);
-                        mma_bf16(tmem + (uint32_t)(b * 32), da, dbd, id, (i > 0 || s > 0) ? 1u : 0u);
+                for (int dx = 0; dx < 3; dx++) {
+                    const uint64_t da = sdesc(pb + s * 2 * kRowQ + dx * 16, kRowQ, PW * 16);
+                    mma_bf16(tmem + (uint32_t)(dx * 32), da, dz, id, (i > 0 || s > 0) ? 1u : 0u);
+                }
+            }
+            mma_commit(&done[b]);
+            last_mma = i;
+        }
+        // bias gradient from the dZ tile: per instruction a warp reads 32
+        // consecutive words (8 pixels x 16 B), no bank conflicts
+        const unsigned char *zt = sm + b * kWgStage + kWgPatchBuf;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+#pragma unroll
+            for (int pb8 = 0; pb8 < 4; pb8++) {
+                const int px = warp * 32 + pb8 * 8 + (lane >> 2);
+                const __nv_bfloat162 v =
+                    *reinterpret_cast<const __nv_bfloat162 *>(zt + q * kZPlane + px * 16 + (lane & 3) * 4);
+                dbp[2 * q] += __low2float(v);
+                dbp[2 * q + 1] += __high2float(v);
+            }
+        }
+        fence_async_smem();  // this stage's generic reads before a later TMA write into it
+        __syncthreads();
+    }
+    const int n = i;  // iterations entered (the last may have failed)
+    if (failed) {
+        if (tid == 0) {
+            atomicExch(&g_corr_err, 1);
+            // whatever may still run: the last load and the last MMAs
+            if (last_load >= 0) mbar_wait(&full[last_load & 1], (last_load >> 1) & 1);
+            if (last_mma >= 0) mbar_wait(&done[last_mma & 1], (last_mma >> 1) & 1);
+        }
+    } else if (n > 0) {
+        const int L = n - 1;
+        const bool ok = mbar_wait(&done[L & 1], (L >> 1) & 1);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(&g_corr_err, 1);
+        } else {
+            fence_after();
+            if (warp < 3) {  // rows 0..95: dy = warp, cin = lane; rows 96..127 are ignored
+#pragma unroll 1
+                for (int dx = 0; dx < 3; dx++) {
+                    float v[32];
+                    tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(dx * 32), v);
+                    const int m = (warp * 3 + dx) * 32 + lane;  // tap * 32 + cin
+#pragma unroll
+                    for (int c = 0; c < 32; c++) atomicAdd(dW + c * KROWS + m, v[c]);
+                }
+            }
+            if (db) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    float v = dbp[k];
+                    v += __shfl_xor_sync(0xffffffffu, v, 4);
+                    v += __shfl_xor_sync(0xffffffffu, v, 8);
+                    v += __shfl_xor_sync(0xffffffffu, v, 16);
+                    dbp[k] = v;
+                }
+                if (lane < 4) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        atomicAdd(db + q * 8 + 2 * lane, dbp[2 * q]);
+                        atomicAdd(db + q * 8 + 2 * lane + 1, dbp[2 * q + 1]);
                     }
                 }
-                mma_commit(mbar);
-            }
-            // the A buffer is rewritten by the next round: wait for these MMAs
-            const bool ok = mbar_wait(mbar, nwait & 1);
-            nwait++;
-            if (__syncthreads_or(!ok)) {
-                failed = true;
-                if (tid == 0) atomicExch(&g_corr_err, 1);
-                mbar_wait(mbar, (nwait - 1) & 1);
-            }
-            fence_after();
-        }
-        if (failed) break;
-    }
-    if (!failed && i > 0) {
-#pragma unroll 1
-        for (int b = 0; b < 3; b++) {
-            float v[32];
-            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(b * 32), v);
-            const int m = b * 128 + warp * 32 + lane;
-            if (m < KROWS) {
-#pragma unroll
-                for (int n = 0; n < 32; n++) atomicAdd(dW + n * KROWS + m, v[n]);
-            } else if (m == KROWS && db) {
-#pragma unroll
-                for (int n = 0; n < 32; n++) atomicAdd(db + n, v[n]);
             }
         }
     }
@@ -667,15 +705,33 @@ cudaError_t conv_launch(const ConvArgs &a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// The NHWC tensor viewed as [n][y][channel quarter][x][8 channels] (dims
+// innermost first: 8 channels, x at 64 B, quarter at 16 B, y, n): a PW x PH
+// box lands in shared memory as [row][quarter][x][8], the weight gradient's
+// A operand layout.
+cudaError_t make_map_rowq(CUtensorMap *m, const void *base, int nimg, int H, int W) {
+    EncodeTiledFn f = tensor_map_encoder();
+    if (!f) return cudaErrorNotSupported;
+    const cuuint64_t dims[5] = {8, (cuuint64_t)W, 4, (cuuint64_t)H, (cuuint64_t)nimg};
+    const cuuint64_t strides[4] = {(cuuint64_t)C * 2, 16, (cuuint64_t)C * 2 * W, (cuuint64_t)C * 2 * W * H};
+    const cuuint32_t box[5] = {8, (cuuint32_t)PW, 4, (cuuint32_t)PH, 1};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    const CUresult r = f(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(base), dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 cudaError_t wgrad_launch(const bf16 *X, const bf16 *dZ, int nimg, int H, int W, float *dW, float *db, cudaStream_t st) {
     cudaError_t e = prepare();
     if (e != cudaSuccess) return e;
     if (reinterpret_cast<uintptr_t>(X) % 16 || reinterpret_cast<uintptr_t>(dZ) % 16) return cudaErrorInvalidValue;
     CUtensorMap mx, mz;
-    e = make_map(&mx, X, nimg, H, W, PW, PH);
+    e = make_map_rowq(&mx, X, nimg, H, W);
     if (e == cudaSuccess) e = make_map(&mz, dZ, nimg, H, W, TXP, TYP);
     if (e != cudaSuccess) return e;
     const TileGeom G = tile_geom(nimg, H, W);
+    // 4 persistent CTAs per SM: 128 TMEM columns each
     const int ctas = std::min(G.total, kWgCtasPerSm * num_sms());
     conv3x3_wgrad_kernel<<<ctas, 128, kWgSmem, st>>>(mx, mz, nimg, H, W, dW, db);
     return cudaGetLastError();
