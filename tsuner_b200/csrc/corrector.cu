@@ -73,8 +73,11 @@ constexpr int kPatch = 4 * kPlane;          // 11776 B
 constexpr int kWBytes = 9 * 4 * 32 * 16;    // weights: 18432 B
 constexpr int KROWS = 9 * C;                // 288
 
-constexpr int kFwdSmem = 1024 + kWBytes + 2 * kPatch + 64;
-constexpr int kFwdCtasPerSm = 5;  // 5 x (43 KB + 1 KB) of shared memory, 5 x 64 TMEM columns
+// patch buffers: tile i+1 loads while tile i's MMAs run and tile i-1's
+// epilogue stages its output in the buffer tile i-1 was read from
+constexpr int kFwdBufs = 3;
+constexpr int kFwdSmem = 1024 + kWBytes + kFwdBufs * kPatch + 64;
+constexpr int kFwdCtasPerSm = 4;  // 4 x (54 KB + 1 KB) of shared memory, 4 x 64 TMEM columns
 static_assert(kFwdCtasPerSm * (kFwdSmem + 1024) <= 228 * 1024 && kFwdCtasPerSm * 64 <= 512, "fwd residency");
 static_assert(kPlane % 128 == 0 && kPlane >= kPlaneData && kWBytes % 128 == 0, "TMA destinations");
 // wgrad: patch + dZ tile + A for half of the 8 K steps (4 x 3 M blocks x 4 KB);
@@ -292,10 +295,11 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __gr
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = smem_align<1024>(sm_raw);
     unsigned char *sW = sm;
-    unsigned char *sP[2] = {sm + kWBytes, sm + kWBytes + kPatch};
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + kWBytes + 2 * kPatch);  // [2] MMA done, [2] patch loaded
-    uint64_t *full = mbar + 2;
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 4);
+    unsigned char *sP0 = sm + kWBytes;  // kFwdBufs patch buffers
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sP0 + kFwdBufs * kPatch);  // [2] MMA done (per TMEM slot)
+    uint64_t *full = mbar + 2;                                               // [kFwdBufs] patch loaded
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(full + kFwdBufs);
+    static_assert((2 + kFwdBufs) * 8 + 4 <= 64, "barriers");
     __shared__ float sBias[32];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TileGeom G = tile_geom(a.nimg, a.H, a.W);
@@ -309,7 +313,7 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __gr
     if (tid < 32) sBias[tid] = a.bias ? a.bias[tid] : 0.f;
     if (warp == 0) tmem_alloc(tslot, 64);
     if (tid == 0) {
-        for (int k = 0; k < 4; k++) mbar_init(&mbar[k], 1);
+        for (int k = 0; k < 2 + kFwdBufs; k++) mbar_init(&mbar[k], 1);
         mbar_init_fence();
     }
     cp_async_wait_all();  // the weights
@@ -321,16 +325,28 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __gr
     const uint32_t id = idesc(128, 32, 0, 0);
     const uint32_t w_u32 = smem_u32(sW);
 
+    // tile t of iteration k -> patch buffer k % kFwdBufs (tid 0)
+    auto load = [&](int t, int k) {
+        const int img = t / G.per_img, r = t - img * G.per_img;
+        const int tyi = r / G.ntx, txi = r - tyi * G.ntx;
+        const int b = k % kFwdBufs;
+        mbar_expect_tx(&full[b], 4 * kPlaneData);
+        issue_patch(&tmX, img, txi * TXP, tyi * TYP, sP0 + b * kPatch, &full[b]);
+    };
+    int issued = -1, consumed = -1;  // iterations whose load tid 0 issued / waited for
+    if (tid == 0 && (int)blockIdx.x < G.total) {
+        load(blockIdx.x, 0);
+        issued = 0;
+    }
     bool failed = false;
-    int prev = -1, i = 0, last_load = -1;
+    int prev = -1, i = 0;
     for (int t = blockIdx.x;; t += gridDim.x, i++) {
         const bool have = t < G.total;
-        if (have && tid == 0) {  // the patch buffer's previous MMAs finished (waited below one tile ago)
-            const int img = t / G.per_img, r = t - img * G.per_img;
-            const int tyi = r / G.ntx, txi = r - tyi * G.ntx;
-            mbar_expect_tx(&full[i & 1], 4 * kPlaneData);
-            issue_patch(&tmX, img, txi * TXP, tyi * TYP, sP[i & 1], &full[i & 1]);
-            last_load = i;
+        // tile i+1 into buffer (i+1) % 3: it held tile i-2, whose MMAs and
+        // epilogue finished before the last barrier
+        if (have && tid == 0 && t + (int)gridDim.x < G.total) {
+            load(t + gridDim.x, i + 1);
+            issued = i + 1;
         }
         if (prev >= 0) {  // epilogue of the previous tile overlaps this tile's loads
             const int j = i - 1;
@@ -343,15 +359,17 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __gr
             // the staging area is the patch buffer of tile j, whose MMAs are done;
             // the next TMA load into it comes after the barrier below (the proxy
             // fence orders these generic accesses before that async write)
-            conv_epilogue(a, G, prev, tmem + (uint32_t)((j & 1) * 32), warp, lane, sBias, sP[j & 1]);
+            conv_epilogue(a, G, prev, tmem + (uint32_t)((j & 1) * 32), warp, lane, sBias,
+                          sP0 + (j % kFwdBufs) * kPatch);
             fence_async_smem();
         }
         if (!have) break;
         fence_before();
         __syncthreads();
         fence_after();
-        if (tid == 0 && mbar_wait(&full[i & 1], (i >> 1) & 1)) {
-            const uint32_t p_u32 = smem_u32(sP[i & 1]);
+        if (tid == 0 && mbar_wait(&full[i % kFwdBufs], (i / kFwdBufs) & 1)) {
+            consumed = i;
+            const uint32_t p_u32 = smem_u32(sP0 + (i % kFwdBufs) * kPatch);
             const uint32_t d = tmem + (uint32_t)((i & 1) * 32);
 #pragma unroll 1
             for (int tap = 0; tap < 9; tap++) {
@@ -370,8 +388,8 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __gr
     if (failed) {
         if (tid == 0) {
             atomicExch(&g_corr_err, 1);
-            // the patch load of this tile may still run: wait for it once more
-            if (last_load >= 0) mbar_wait(&full[last_load & 1], (last_load >> 1) & 1);
+            // patch loads that may still run: issued but not waited for
+            for (int k = consumed + 1; k <= issued; k++) mbar_wait(&full[k % kFwdBufs], (k / kFwdBufs) & 1);
         }
         // the MMAs of the last issued tile may still run
         mbar_wait(&mbar[(i - 1) & 1], ((i - 1) >> 1) & 1);
@@ -698,8 +716,7 @@ cudaError_t conv_launch(const ConvArgs &a, cudaStream_t st) {
     e = make_map(&mx, a.X, a.nimg, a.H, a.W, PW, PH);
     if (e != cudaSuccess) return e;
     const TileGeom G = tile_geom(a.nimg, a.H, a.W);
-    // 5 persistent CTAs per SM (43 KB of shared memory and 64 TMEM columns each;
-    // measured 16 % faster than 4)
+    // persistent CTAs, kFwdCtasPerSm per SM (shared memory and TMEM bound)
     const int ctas = std::min(G.total, kFwdCtasPerSm * num_sms());
     conv3x3_fwd_kernel<<<ctas, 128, kFwdSmem, st>>>(a, mx);
     return cudaGetLastError();
