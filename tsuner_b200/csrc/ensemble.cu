@@ -118,8 +118,8 @@ int build_tables(TsuEnsemble *E, int variant) {
     const bool tma_allowed = !(tma_env && tma_env[0] == '0');
     for (int i = 0; i < E->n; i++) {
         TsuSolver *s = E->m[i];
-        tmas[i].on = tma_allowed && stage32_tma_maps(variant, (const float *)s->A, (const float *)s->B, s->pitch,
-                                                     s->plane, s->p.npx, s->p.npy, &tmas[i].a, &tmas[i].b);
+        tmas[i].on = tma_allowed && stage32_tma_maps(variant, (const float *)s->A, (const float *)s->B, s->mask,
+                                                     s->pitch, s->plane, s->p.npx, s->p.npy, &tmas[i]);
     }
     cudaFree(E->d_members);
     cudaFree(E->d_tile_member);

@@ -227,11 +227,19 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
     // TSU_STAGE_TMA=0 makes every tile load with ordinary instructions
     const char *tma_env = std::getenv("TSU_STAGE_TMA");
     const bool tma_allowed = !(tma_env && tma_env[0] == '0');
-    if (e == cudaSuccess && tma_allowed)
-        s->tma = s->fp32 ? stage32_tma_maps(-1, (const float *)s->A, (const float *)s->B, s->pitch, s->plane, p->npx,
-                                            p->npy, &s->tmA, &s->tmB)
-                         : stage64_tma_maps((const double *)s->A, (const double *)s->B, s->pitch, s->plane, p->npx,
-                                            p->npy, &s->tmA, &s->tmB);
+    if (e == cudaSuccess && tma_allowed) {
+        if (s->fp32) {
+            Tma32 t32{};
+            s->tma = stage32_tma_maps(-1, (const float *)s->A, (const float *)s->B, s->mask, s->pitch, s->plane,
+                                      p->npx, p->npy, &t32);
+            s->tmA = t32.a;
+            s->tmB = t32.b;
+            s->tmM = t32.m;
+        } else {
+            s->tma = stage64_tma_maps((const double *)s->A, (const double *)s->B, s->pitch, s->plane, p->npx, p->npy,
+                                      &s->tmA, &s->tmB);
+        }
+    }
     if (e != cudaSuccess) {
         int r = cuda_fail(e, "tsu_create");
         free_all(s);
@@ -446,6 +454,7 @@ int TsuSolver::launch_steps(long n) {
         Tma32 tm;
         tm.a = tmA;
         tm.b = tmB;
+        tm.m = tmM;
         tm.on = tma ? 1 : 0;
         for (long i = 0; i < n; i++)
             for (int k = 0; k < sw.order; k++) CK(stage32_launch(sw.order, k, a, tm, st));

@@ -35,8 +35,12 @@ struct T32 {
     static constexpr int kFx = 12 * TY * FXW, kFy = 12 * FYH * TX;  // 2 faces x 6 floats
     static constexpr int kDeta = 2 * TY * TX, kWarps = NT / 32;
     static constexpr int kFloats = kRegA + kFx + kFy + kDeta;
+    // the 1-byte mask: rows of MLX = TX + 32 cells starting 16 left of the
+    // tile (a 16-byte aligned TMA origin for bytes), 128-byte aligned
+    static constexpr int MHX = 16, MLX = TX + 2 * MHX, MPS = MLX * LY;
+    static constexpr size_t kMaskOff = (sizeof(float) * kFloats + sizeof(double) * 3 * kWarps + 127) / 128 * 128;
     // + 128: the base is rounded up to 128 bytes (TMA destination)
-    static constexpr size_t smem() { return sizeof(float) * kFloats + sizeof(double) * 3 * kWarps + PS + 64 + 128; }
+    static constexpr size_t smem() { return kMaskOff + MPS + 64 + 128; }
 };
 
 __device__ __forceinline__ int wrap_clamp32(int g, int n, bool periodic) {
@@ -129,7 +133,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
                                              unsigned blin, unsigned nb, float *smem_raw) {
     using T = T32<TX, TY>;
     constexpr int NT = T::NT, LX = T::LX, PS = T::PS, FXW = T::FXW, FYH = T::FYH, kWarps = T::kWarps;
-    constexpr int HX = T::HX, LXC = T::LXC, PSC = T::PSC;
+    constexpr int HX = T::HX, LXC = T::LXC, PSC = T::PSC, MHX = T::MHX, MLX = T::MLX;
     float *smem32 = smem_align<128>(smem_raw);
     __shared__ uint64_t sBar;  // the tile's TMA load
     float *sV = smem32;
@@ -138,7 +142,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     float *sFy = sFx + T::kFx;
     float *sDeta = sFy + T::kFy;
     double *sRed = reinterpret_cast<double *>(sDeta + T::kDeta);  // [3][kWarps]
-    unsigned char *sM = reinterpret_cast<unsigned char *>(sRed + 3 * kWarps);
+    unsigned char *sM = reinterpret_cast<unsigned char *>(smem32) + T::kMaskOff;
     __shared__ int sLast;
 
     // Global memory is accessed through explicit global-space loads and
@@ -183,23 +187,24 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     if (use_tma && tid == 0) {
         mbar_init(&sBar, 1);
         mbar_init_fence();
-        mbar_expect_tx(&sBar, 5 * PS * sizeof(float));
+        mbar_expect_tx(&sBar, 5 * PS * sizeof(float) + T::MPS);
         tma_load_3d(sV, (Vin == A.bufB) ? &tm->b : &tm->a, x0 - HX, y0 - 2, 0, &sBar);
+        tma_load_2d(sM, &tm->m, x0 - MHX, y0 - 2, &sBar);
     }
-    for (int k = tid; k < PSC; k += NT) {
-        const int ly = k / LXC, lxc = k - ly * LXC;
-        const int idx = ly * LX + lxc + (HX - 2);
-        int gx = x0 + lxc - 2, gy = y0 + ly - 2;
-        if (!inner) {
-            gx = wrap_clamp32(gx, npx, periodic);
-            gy = wrap_clamp32(gy, npy, periodic);
-        }
-        const long long g = (long long)gy * pitch + gx;
-        if (!use_tma) {
+    if (!use_tma) {
+        for (int k = tid; k < PSC; k += NT) {
+            const int ly = k / LXC, lxc = k - ly * LXC;
+            const int idx = ly * LX + lxc + (HX - 2);
+            int gx = x0 + lxc - 2, gy = y0 + ly - 2;
+            if (!inner) {
+                gx = wrap_clamp32(gx, npx, periodic);
+                gy = wrap_clamp32(gy, npy, periodic);
+            }
+            const long long g = (long long)gy * pitch + gx;
 #pragma unroll
             for (int f = 0; f < 5; f++) sV[f * PS + idx] = __ldg(Vin + f * plane + g);
+            sM[ly * MLX + lxc + (MHX - 2)] = __ldg(A.mask + g);
         }
-        sM[idx] = __ldg(A.mask + g);
     }
     const int tx = tid % TX, ty = tid / TX;
     const int gi = x0 + tx, gj = y0 + ty;
@@ -357,13 +362,13 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             if (vert) {
                 a = get_face(sFx + (6 * TY + r) * FXW + e, TY * FXW);
                 b = get_face(sFx + r * FXW + (e + 1), TY * FXW);
-                fixed = (int)sM[(r + 2) * LX + e + HX - 1] * (int)sM[(r + 2) * LX + e + HX];
+                fixed = (int)sM[(r + 2) * MLX + e + MHX - 1] * (int)sM[(r + 2) * MLX + e + MHX];
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
                 if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             } else {
                 a = get_face(sFy + (6 * FYH + e) * TX + c, FYH * TX);
                 b = get_face(sFy + (e + 1) * TX + c, FYH * TX);
-                fixed = (int)sM[(e + 1) * LX + c + HX] * (int)sM[(e + 2) * LX + c + HX];
+                fixed = (int)sM[(e + 1) * MLX + c + MHX] * (int)sM[(e + 2) * MLX + c + MHX];
                 if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
                 if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
             }
@@ -376,7 +381,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             if (periodic && (ex == 0 || ex == npx)) {
                 a = get_face(Rf, TY * FXW);
                 b = get_face(Lf, TY * FXW);
-                fixed = sM[ly * LX + e + HX - 1];
+                fixed = sM[ly * MLX + e + MHX - 1];
                 seam = true;
                 seg = npx + ey;
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
@@ -384,20 +389,20 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             } else if (ex == 0) {
                 a = get_face(Lf, TY * FXW);
                 sgnn = -1;
-                fixed = sM[ly * LX + e + HX];
+                fixed = sM[ly * MLX + e + MHX];
                 bnd = true;
                 seg = 2 * npx + npy + ey;
                 outM = sFlux + 0 * 5 * FS + r * TX + e;
             } else if (ex == npx) {
                 a = get_face(Rf, TY * FXW);
-                fixed = sM[ly * LX + e + HX - 1];
+                fixed = sM[ly * MLX + e + MHX - 1];
                 bnd = true;
                 seg = npx + ey;
                 outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
             } else {
                 a = get_face(Rf, TY * FXW);
                 b = get_face(Lf, TY * FXW);
-                fixed = (int)sM[ly * LX + e + HX - 1] * (int)sM[ly * LX + e + HX];
+                fixed = (int)sM[ly * MLX + e + MHX - 1] * (int)sM[ly * MLX + e + MHX];
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
                 if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             }
@@ -409,7 +414,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             if (periodic && (ey == 0 || ey == npy)) {
                 a = get_face(Uf, FYH * TX);
                 b = get_face(Df, FYH * TX);
-                fixed = sM[(e + 1) * LX + c + HX];
+                fixed = sM[(e + 1) * MLX + c + MHX];
                 seam = true;
                 seg = npx + npy + ex;
                 if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
@@ -417,20 +422,20 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             } else if (ey == 0) {
                 a = get_face(Df, FYH * TX);
                 sgnn = -1;
-                fixed = sM[(e + 2) * LX + c + HX];
+                fixed = sM[(e + 2) * MLX + c + MHX];
                 bnd = true;
                 seg = ex;
                 outM = sFlux + 2 * 5 * FS + e * TX + c;
             } else if (ey == npy) {
                 a = get_face(Uf, FYH * TX);
-                fixed = sM[(e + 1) * LX + c + HX];
+                fixed = sM[(e + 1) * MLX + c + MHX];
                 bnd = true;
                 seg = npx + npy + ex;
                 outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
             } else {
                 a = get_face(Uf, FYH * TX);
                 b = get_face(Df, FYH * TX);
-                fixed = (int)sM[(e + 1) * LX + c + HX] * (int)sM[(e + 2) * LX + c + HX];
+                fixed = (int)sM[(e + 1) * MLX + c + MHX] * (int)sM[(e + 2) * MLX + c + MHX];
                 if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
                 if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
             }
@@ -859,8 +864,8 @@ int which(int order, int stage) { return (order == 2) ? (stage == 0 ? 0 : 1) : 2
 
 }  // namespace
 
-bool stage32_tma_maps(int variant, const float *bufA, const float *bufB, long long pitch, long long plane, int npx,
-                      int npy, CUtensorMap *tmA, CUtensorMap *tmB) {
+bool stage32_tma_maps(int variant, const float *bufA, const float *bufB, const unsigned char *mask, long long pitch,
+                      long long plane, int npx, int npy, Tma32 *out) {
     EncodeTiledFn f = tensor_map_encoder();
     int nv;
     variants32(&nv);
@@ -868,19 +873,29 @@ bool stage32_tma_maps(int variant, const float *bufA, const float *bufB, long lo
     if (variant >= nv) return false;
     const Variant32 &v = variants32(nullptr)[variant];
     const int lx = v.tx + 8, ly = v.ty + 4;  // T32<TX, TY>::LX, LY
+    const int mlx = v.tx + 32;               // T32<TX, TY>::MLX
     if (!f || npx < lx || npy < ly) return false;
-    if (reinterpret_cast<uintptr_t>(bufA) % 16 || reinterpret_cast<uintptr_t>(bufB) % 16) return false;
+    if (reinterpret_cast<uintptr_t>(bufA) % 16 || reinterpret_cast<uintptr_t>(bufB) % 16 ||
+        reinterpret_cast<uintptr_t>(mask) % 16 || pitch % 16)
+        return false;
     const cuuint64_t dims[3] = {(cuuint64_t)npx, (cuuint64_t)npy, 5};
     const cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(float), (cuuint64_t)plane * sizeof(float)};
     const cuuint32_t box[3] = {(cuuint32_t)lx, (cuuint32_t)ly, 5};
     const cuuint32_t es[3] = {1, 1, 1};
     const float *bufs[2] = {bufA, bufB};
-    CUtensorMap *maps[2] = {tmA, tmB};
+    CUtensorMap *maps[2] = {&out->a, &out->b};
     for (int k = 0; k < 2; k++)
         if (f(maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(bufs[k]), dims, strides, box, es,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return false;
+    const cuuint64_t mdims[2] = {(cuuint64_t)npx, (cuuint64_t)npy};
+    const cuuint64_t mstrides[1] = {(cuuint64_t)pitch};
+    const cuuint32_t mbox[2] = {(cuuint32_t)mlx, (cuuint32_t)ly};
+    if (f(&out->m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<unsigned char *>(mask), mdims, mstrides, mbox, es,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
     return true;
 }
 

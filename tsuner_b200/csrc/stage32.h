@@ -37,6 +37,7 @@ struct EnsMember {
 // [5][npy][npx] (boxes = the loaded tile); `on` = 0 means ordinary loads.
 struct Tma32 {
     CUtensorMap a, b;
+    CUtensorMap m;  // the uint8 mask [npy][pitch] (box origin x0 - 16: 16-byte aligned)
     int on;
 };
 
@@ -57,8 +58,8 @@ dim3 stage32_grid(int npx, int npy);
 cudaError_t stage32_launch(int order, int stage, const Stage32Args &a, const Tma32 &tm, cudaStream_t st);
 // TMA descriptors of two FP32 state buffers with the boxes of tile variant
 // `variant` (-1: the single-grid variant); false if they cannot be made
-bool stage32_tma_maps(int variant, const float *bufA, const float *bufB, long long pitch, long long plane, int npx,
-                      int npy, CUtensorMap *tmA, CUtensorMap *tmB);
+bool stage32_tma_maps(int variant, const float *bufA, const float *bufB, const unsigned char *mask, long long pitch,
+                      long long plane, int npx, int npy, Tma32 *out);
 // tile-shape variants available to the ensemble kernel
 int stage32_num_tiles();
 void stage32_tile_shape(int variant, int *tx, int *ty, int *minb);
