@@ -236,8 +236,8 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
             s->tmB = t32.b;
             s->tmM = t32.m;
         } else {
-            s->tma = stage64_tma_maps((const double *)s->A, (const double *)s->B, s->pitch, s->plane, p->npx, p->npy,
-                                      &s->tmA, &s->tmB);
+            s->tma = stage64_tma_maps((const double *)s->A, (const double *)s->B, s->mask, s->pitch, s->plane, p->npx,
+                                      p->npy, &s->tmA, &s->tmB, &s->tmM);
         }
     }
     if (e != cudaSuccess) {
@@ -390,6 +390,7 @@ Stage64Args TsuSolver::args() const {
     a.phys = phys;
     a.tmA = tmA;
     a.tmB = tmB;
+    a.tmM = tmM;
     a.tma = tma ? 1 : 0;
     return a;
 }

@@ -37,7 +37,7 @@ struct TsuSolver {
     bool has_state = false, ready = false, timed = false;
     // TMA descriptors of A and B (interior tiles stage their loads by TMA)
     CUtensorMap tmA{}, tmB{};
-    CUtensorMap tmM{};  // FP32 form: the mask
+    CUtensorMap tmM{};  // the mask (uint8 [npy][pitch])
     bool tma = false;
 
     tsu::Stage64Args args() const;

@@ -48,8 +48,12 @@ struct Tile {
     static constexpr int kRegA = (kSV + kSUC) > kFlux ? (kSV + kSUC) : kFlux;
     static constexpr int kFx = 10 * TY * FXW, kFy = 10 * FYH * TX, kDeta = 2 * TY * TX, kRed = NT / 32;
     static constexpr int kDoubles = kRegA + kFx + kFy + kDeta + kRed;
+    // the 1-byte mask: rows of MLX = TX + 32 cells starting 16 left of the
+    // tile (a 16-byte aligned TMA origin for bytes), 128-byte aligned
+    static constexpr int MHX = 16, MLX = TX + 2 * MHX, MPS = MLX * LY;
+    static constexpr size_t kMaskOff = (sizeof(double) * kDoubles + 127) / 128 * 128;
     // + 128: the base is rounded up to 128 bytes (TMA destination)
-    static constexpr size_t smem() { return sizeof(double) * kDoubles + PS + 16 + 128; }
+    static constexpr size_t smem() { return kMaskOff + MPS + 16 + 128; }
 };
 
 __device__ __forceinline__ int wrap_clamp(int g, int n, bool periodic) {
@@ -139,6 +143,7 @@ template <int TX, int TY, int NTHR, int MINB, int ORDER, bool FIRST, bool LAST>
 __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_constant__ Stage64Args A) {
     using T = Tile<TX, TY, NTHR>;
     constexpr int NT = T::NT, LX = T::LX, LY = T::LY, PS = T::PS, FXW = T::FXW, FYH = T::FYH;
+    constexpr int MHX = T::MHX, MLX = T::MLX;
     extern __shared__ __align__(16) double smem_raw[];
     double *smem = smem_align<128>(smem_raw);
     __shared__ uint64_t sBar;  // the tile's TMA load
@@ -150,7 +155,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
     double *sFy = sFx + T::kFx;         // [2][5][FYH][TX]
     double *sDeta = sFy + T::kFy;       // [2][TY][TX]
     double *sRed = sDeta + T::kDeta;    // [NT/32]
-    unsigned char *sM = reinterpret_cast<unsigned char *>(sRed + T::kRed);  // [LY][LX]
+    unsigned char *sM = reinterpret_cast<unsigned char *>(smem) + T::kMaskOff;  // [LY][MLX], tile at column MHX
     __shared__ int sLast;
 
     const double t = A.scal[SC_T];
@@ -183,19 +188,17 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
     const bool inner = !periodic && x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= npx && y0 + TY + 2 <= npy;
 
     // ---- phase 1: tile + halo -> smem.  Interior tiles: one TMA box of the
-    // 5 state planes (x0 - 2 doubles = a multiple of 16 bytes); the mask and
-    // boundary tiles (clamped or wrapped halo) with ordinary loads.
+    // 5 state planes (x0 - 2 doubles = a multiple of 16 bytes) and one of the
+    // mask (from x0 - 16); boundary tiles (clamped or wrapped halo) with
+    // ordinary loads.
     const bool use_tma = inner && A.tma;
     if (use_tma) {
         if (tid == 0) {
             mbar_init(&sBar, 1);
             mbar_init_fence();
-            mbar_expect_tx(&sBar, 5 * PS * sizeof(double));
+            mbar_expect_tx(&sBar, 5 * PS * sizeof(double) + T::MPS);
             tma_load_3d(sV, (Vin == A.bufB) ? &A.tmB : &A.tmA, x0 - 2, y0 - 2, 0, &sBar);
-        }
-        for (int idx = tid; idx < PS; idx += NT) {
-            const int ly = idx / LX, lx = idx - ly * LX;
-            sM[idx] = A.mask[(long long)(y0 + ly - 2) * pitch + (x0 + lx - 2)];
+            tma_load_2d(sM, &A.tmM, x0 - MHX, y0 - 2, &sBar);
         }
     } else {
         for (int idx = tid; idx < PS; idx += NT) {
@@ -208,7 +211,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             const long long g = (long long)gy * pitch + gx;
 #pragma unroll
             for (int f = 0; f < 5; f++) sV[f * PS + idx] = Vin[f * plane + g];
-            sM[idx] = A.mask[g];
+            sM[ly * MLX + lx + (MHX - 2)] = A.mask[g];
         }
     }
     const bool cell_thread = tid < TX * TY;  // owns a cell in the update
@@ -311,7 +314,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
                 const int r = item / (TX + 1), e = item - r * (TX + 1);
                 a = get5(sFx + (5 * TY + r) * FXW + e, TY * FXW);
                 b = get5(sFx + r * FXW + (e + 1), TY * FXW);
-                fixed = (int)sM[(r + 2) * LX + e + 1] * (int)sM[(r + 2) * LX + e + 2];
+                fixed = (int)sM[(r + 2) * MLX + e + 1 + (MHX - 2)] * (int)sM[(r + 2) * MLX + e + 2 + (MHX - 2)];
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
                 if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             } else {
@@ -322,7 +325,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
                 const int e = it / TX, c = it - e * TX;
                 a = get5(sFy + (5 * FYH + e) * TX + c, FYH * TX);
                 b = get5(sFy + (e + 1) * TX + c, FYH * TX);
-                fixed = (int)sM[(e + 1) * LX + c + 2] * (int)sM[(e + 2) * LX + c + 2];
+                fixed = (int)sM[(e + 1) * MLX + c + 2 + (MHX - 2)] * (int)sM[(e + 2) * MLX + c + 2 + (MHX - 2)];
                 if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
                 if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
             }
@@ -340,7 +343,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             if (periodic && (ex == 0 || ex == npx)) {  // seam: GPU/VolumeSolver.cu:262-275,289-298
                 a = get5(Rf, TY * FXW);
                 b = get5(Lf, TY * FXW);
-                fixed = sM[ly * LX + e + 1];
+                fixed = sM[ly * MLX + e + 1 + (MHX - 2)];
                 seam = true;
                 seg = npx + ey;
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
@@ -348,20 +351,20 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             } else if (ex == 0) {  // west: GPU/VolumeSolver.cu:233-258
                 a = get5(Lf, TY * FXW);
                 nx = -1;
-                fixed = sM[ly * LX + e + 2];
+                fixed = sM[ly * MLX + e + 2 + (MHX - 2)];
                 bnd = true;
                 seg = 2 * npx + npy + ey;
                 outM = sFlux + 0 * 5 * FS + r * TX + e;
             } else if (ex == npx) {  // east: GPU/VolumeSolver.cu:276-298
                 a = get5(Rf, TY * FXW);
-                fixed = sM[ly * LX + e + 1];
+                fixed = sM[ly * MLX + e + 1 + (MHX - 2)];
                 bnd = true;
                 seg = npx + ey;
                 outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
             } else {  // interior: GPU/VolumeSolver.cu:300-314
                 a = get5(Rf, TY * FXW);
                 b = get5(Lf, TY * FXW);
-                fixed = (int)sM[ly * LX + e + 1] * (int)sM[ly * LX + e + 2];
+                fixed = (int)sM[ly * MLX + e + 1 + (MHX - 2)] * (int)sM[ly * MLX + e + 2 + (MHX - 2)];
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
                 if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             }
@@ -379,7 +382,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             if (periodic && (ey == 0 || ey == npy)) {  // seam: GPU/VolumeSolver.cu:352-367,378-387
                 a = get5(Uf, FYH * TX);
                 b = get5(Df, FYH * TX);
-                fixed = sM[(e + 1) * LX + c + 2];
+                fixed = sM[(e + 1) * MLX + c + 2 + (MHX - 2)];
                 seam = true;
                 seg = npx + npy + ex;
                 if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
@@ -387,20 +390,20 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             } else if (ey == 0) {  // south: GPU/VolumeSolver.cu:324-349
                 a = get5(Df, FYH * TX);
                 ny = -1;
-                fixed = sM[(e + 2) * LX + c + 2];
+                fixed = sM[(e + 2) * MLX + c + 2 + (MHX - 2)];
                 bnd = true;
                 seg = ex;
                 outM = sFlux + 2 * 5 * FS + e * TX + c;
             } else if (ey == npy) {  // north: GPU/VolumeSolver.cu:352-387
                 a = get5(Uf, FYH * TX);
-                fixed = sM[(e + 1) * LX + c + 2];
+                fixed = sM[(e + 1) * MLX + c + 2 + (MHX - 2)];
                 bnd = true;
                 seg = npx + npy + ex;
                 outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
             } else {  // interior: GPU/VolumeSolver.cu:389-403
                 a = get5(Uf, FYH * TX);
                 b = get5(Df, FYH * TX);
-                fixed = (int)sM[(e + 1) * LX + c + 2] * (int)sM[(e + 2) * LX + c + 2];
+                fixed = (int)sM[(e + 1) * MLX + c + 2 + (MHX - 2)] * (int)sM[(e + 2) * MLX + c + 2 + (MHX - 2)];
                 if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
                 if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
             }
@@ -677,12 +680,14 @@ cudaError_t stage64_prepare() {
     return cudaSuccess;
 }
 
-bool stage64_tma_maps(const double *bufA, const double *bufB, long long pitch, long long plane, int npx, int npy,
-                      CUtensorMap *tmA, CUtensorMap *tmB) {
+bool stage64_tma_maps(const double *bufA, const double *bufB, const unsigned char *mask, long long pitch, long long plane,
+                      int npx, int npy, CUtensorMap *tmA, CUtensorMap *tmB, CUtensorMap *tmM) {
     EncodeTiledFn f = tensor_map_encoder();
     const Variant &v = variant();
     if (!f || npx < v.tx + 4 || npy < v.ty + 4) return false;
-    if (reinterpret_cast<uintptr_t>(bufA) % 16 || reinterpret_cast<uintptr_t>(bufB) % 16) return false;
+    if (reinterpret_cast<uintptr_t>(bufA) % 16 || reinterpret_cast<uintptr_t>(bufB) % 16 ||
+        reinterpret_cast<uintptr_t>(mask) % 16 || pitch % 16)
+        return false;
     const cuuint64_t dims[3] = {(cuuint64_t)npx, (cuuint64_t)npy, 5};
     const cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(double), (cuuint64_t)plane * sizeof(double)};
     const cuuint32_t box[3] = {(cuuint32_t)(v.tx + 4), (cuuint32_t)(v.ty + 4), 5};
@@ -694,6 +699,13 @@ bool stage64_tma_maps(const double *bufA, const double *bufB, long long pitch, l
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return false;
+    const cuuint64_t mdims[2] = {(cuuint64_t)npx, (cuuint64_t)npy};
+    const cuuint64_t mstrides[1] = {(cuuint64_t)pitch};
+    const cuuint32_t mbox[2] = {(cuuint32_t)(v.tx + 32), (cuuint32_t)(v.ty + 4)};  // Tile::MLX, LY
+    if (f(tmM, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<unsigned char *>(mask), mdims, mstrides, mbox, es,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
     return true;
 }
 

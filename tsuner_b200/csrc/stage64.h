@@ -29,6 +29,7 @@ struct Stage64Args {
     // (boxes = the loaded tile with its halo); used for tiles whose halo lies
     // inside the grid when `tma` is set
     CUtensorMap tmA, tmB;
+    CUtensorMap tmM;  // the uint8 mask [npy][pitch] (box origin x0 - 16)
     int tma;
     double *bufA;           // U^n at step entry (and U^{n+1} at exit, order 2)
     double *bufB;           // U* (order 2) / ping-pong partner (order 1)
@@ -65,7 +66,7 @@ size_t partials_needed(int npx, int npy);
 // encodes the TMA descriptors of the two FP64 state buffers for the current
 // tile shape; false if the driver cannot (the kernels then load with
 // ordinary instructions)
-bool stage64_tma_maps(const double *bufA, const double *bufB, long long pitch, long long plane, int npx, int npy,
-                      CUtensorMap *tmA, CUtensorMap *tmB);
+bool stage64_tma_maps(const double *bufA, const double *bufB, const unsigned char *mask, long long pitch, long long plane,
+                      int npx, int npy, CUtensorMap *tmA, CUtensorMap *tmB, CUtensorMap *tmM);
 
 }  // namespace tsu
