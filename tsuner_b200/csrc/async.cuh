@@ -65,6 +65,9 @@ __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.a
 // bytes complete on `bar`.  The innermost coordinate times the element size
 // must be a multiple of 16 bytes (callers guarantee it); outer coordinates
 // may lie outside the tensor (zero fill).
+// request a line into L2 (no register is written)
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1, uint64_t *bar) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::

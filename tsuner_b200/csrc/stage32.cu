@@ -210,16 +210,17 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     const int gi = x0 + tx, gj = y0 + ty;
     const bool own = (gi < npx) && (gj < npy);
     const long long gown = (long long)(own ? gj : 0) * pitch + (own ? gi : 0);
-    float v0[5];
+    // U^n of the owned cell (second stage) and its running extrema are read
+    // in the update; here they are only requested into L2, so that no
+    // registers are held across the face and edge phases
     if (!FIRST) {
 #pragma unroll
-        for (int f = 0; f < 5; f++) v0[f] = __ldcg(V0 + f * plane + gown);
+        for (int f = 0; f < 5; f++) prefetch_l2(V0 + f * plane + gown);
     }
-    float ex_h = 0.f, ex_b = 0.f, ex_e = 0.f;  // running extrema, loaded early
     if (LAST && own) {
-        ex_h = __ldcg(A.hmax + gown);
-        ex_b = __ldcg(A.bmin + gown);
-        ex_e = __ldcg(A.eta_max + gown);
+        prefetch_l2(A.hmax + gown);
+        prefetch_l2(A.bmin + gown);
+        prefetch_l2(A.eta_max + gown);
     }
     __syncthreads();
     if (use_tma) {  // every thread sees the box land (bounded wait)
@@ -236,10 +237,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     float vc[5];
 #pragma unroll
     for (int f = 0; f < 5; f++) vc[f] = sV[f * PS + cidx];
-    if (FIRST) {
-#pragma unroll
-        for (int f = 0; f < 5; f++) v0[f] = vc[f];
-    }
+
 
     // ---- phase 2: depth, velocity, concentration per cell
     for (int k = tid; k < PSC; k += NT) {
@@ -496,6 +494,15 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     float dtcell = CUDART_INF_F;
     double mass = 0.0, sed = 0.0;
     if (own) {
+        float v0[5];
+#pragma unroll
+        for (int f = 0; f < 5; f++) v0[f] = FIRST ? vc[f] : __ldcg(V0 + f * plane + gown);
+        float ex_h = 0.f, ex_b = 0.f, ex_e = 0.f;
+        if (LAST) {
+            ex_h = __ldcg(A.hmax + gown);
+            ex_b = __ldcg(A.bmin + gown);
+            ex_e = __ldcg(A.eta_max + gown);
+        }
         float z = vc[0], H = vc[1], qx = vc[2], qy = vc[3], hc = vc[4];
         if (ORDER == 2) {
             qx -= dt * P.inv_dx * kGf * hcell * sDeta[ty * TX + tx];
