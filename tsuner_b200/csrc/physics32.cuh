@@ -48,10 +48,12 @@ __device__ __forceinline__ double depth64(float z, float H, double eta0) {
 }
 __device__ __forceinline__ float dry_z(float H, double eta0) { return __double2float_rd(-((double)H + eta0)); }
 
-// u_calculator (GPU/SedFlux.cuh:26-36) in FP32.
-__device__ __forceinline__ void velocity32(float h, float qx, float qy, float &ux, float &uy, float &modu) {
+// u_calculator (GPU/SedFlux.cuh:26-36) in FP32, given r = 1/h (read only
+// when h >= EPS), so that a caller that also divides by h computes the
+// reciprocal once.
+__device__ __forceinline__ void velocity32r(float h, float r, float qx, float qy, float &ux, float &uy,
+                                            float &modu) {
     if (h >= kEpsf) {
-        float r = __frcp_rn(h);
         ux = qx * r;
         uy = qy * r;
         float m2 = ux * ux + uy * uy;
@@ -67,6 +69,10 @@ __device__ __forceinline__ void velocity32(float h, float qx, float qy, float &u
         ux = uy = 0.f;
         modu = 0.f;
     }
+}
+
+__device__ __forceinline__ void velocity32(float h, float qx, float qy, float &ux, float &uy, float &modu) {
+    velocity32r(h, h >= kEpsf ? __frcp_rn(h) : 0.f, qx, qy, ux, uy, modu);
 }
 
 // avg (GPU/Reconstructor.cu:19-31): (a|b| + b|a|)/(|a|+|b|) equals

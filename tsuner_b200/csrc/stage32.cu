@@ -247,11 +247,12 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         const float hs = zz + (P.eta0f + HH);  // FP32 when clearly wet, FP64 near dryness
         const float h = (hs > kWetMarginf) ? hs : (float)depth64(zz, HH, eta0);
         float ux, uy, m;
-        velocity32(h, sV[2 * PS + idx], sV[3 * PS + idx], ux, uy, m);
+        const float rh = (h > 0.f) ? __frcp_rn(h) : 0.f;
+        velocity32r(h, rh, sV[2 * PS + idx], sV[3 * PS + idx], ux, uy, m);
         sV[5 * PS + idx] = h;
         sV[6 * PS + idx] = ux;
         sV[7 * PS + idx] = uy;
-        sV[8 * PS + idx] = (h > 0.f) ? fmaxf(sV[4 * PS + idx] * __frcp_rn(h), 0.f) : 0.f;
+        sV[8 * PS + idx] = (h > 0.f) ? fmaxf(sV[4 * PS + idx] * rh, 0.f) : 0.f;
     }
     __syncthreads();
     const float hcell = sV[5 * PS + cidx];
@@ -512,8 +513,9 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
            // this stage's input, whose depth phase 2 already formed)
             const float h0 = FIRST ? hcell : (float)depth64(v0[0], v0[1], eta0);
             float ux, uy, modu;
-            velocity32(h0, v0[2], v0[3], ux, uy, modu);
-            const float cf = (h0 > 0.f) ? dt * P.FR * modu * __frcp_rn(h0) : 0.f;
+            const float r0 = (h0 > 0.f) ? __frcp_rn(h0) : 0.f;
+            velocity32r(h0, r0, v0[2], v0[3], ux, uy, modu);
+            const float cf = (h0 > 0.f) ? dt * P.FR * modu * r0 : 0.f;
             const float rf = __frcp_rn(1.f + cf);
             qx *= rf;
             qy *= rf;
@@ -556,8 +558,9 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         } else {
             h = (float)hd;
             float m;
-            velocity32(h, qx, qy, uxf, uyf, m);
-            const float c = fmaxf(hc * __frcp_rn(h), 0.f);
+            const float rh = __frcp_rn(h);  // h > 0 here
+            velocity32r(h, rh, qx, qy, uxf, uyf, m);
+            const float c = fmaxf(hc * rh, 0.f);
             qx = h * uxf;
             qy = h * uyf;
             hc = h * c;
