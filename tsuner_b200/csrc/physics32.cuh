@@ -41,6 +41,16 @@ struct Phys32 {
     float grass_ag;
 };
 
+// Reciprocal: the hardware approximation (at most 2 ulp for |x| in
+// [2^-126, 2^126]) refined by one Newton-Raphson step for 1/x,
+// r1 = r0 + r0 (1 - x r0), as two fused multiply-adds.  Every argument here
+// is a normal float (depths and speeds above a positive threshold), so the
+// special-case handling of the correctly rounded __frcp_rn is not needed.
+__device__ __forceinline__ float rcp32(float x) {
+    const float r0 = __fdividef(1.0f, x);
+    return __fmaf_rn(r0, __fmaf_rn(-x, r0, 1.0f), r0);
+}
+
 // Depth from the stored surface deviation (FP64 island), and the stored
 // deviation of a dry cell (rounded down so that z + eta0 + H <= 0 exactly).
 __device__ __forceinline__ double depth64(float z, float H, double eta0) {
@@ -72,7 +82,7 @@ __device__ __forceinline__ void velocity32r(float h, float r, float qx, float qy
 }
 
 __device__ __forceinline__ void velocity32(float h, float qx, float qy, float &ux, float &uy, float &modu) {
-    velocity32r(h, h >= kEpsf ? __frcp_rn(h) : 0.f, qx, qy, ux, uy, modu);
+    velocity32r(h, h >= kEpsf ? rcp32(h) : 0.f, qx, qy, ux, uy, modu);
 }
 
 // avg (GPU/Reconstructor.cu:19-31): (a|b| + b|a|)/(|a|+|b|) equals
@@ -110,7 +120,7 @@ __device__ __forceinline__ float bedload32(const Phys32 &P, float h, float ux, f
     if (P.bedload_law == 1) return -(P.grass_ag * ux * modu * modu / (1.f - P.porosity));
     float O = P.Opar * modu * modu;
     if (O <= P.OC || h <= P.HQB || h <= P.DS5) return 0.f;
-    float K1 = 17.f * ux * __frcp_rn(modu);
+    float K1 = 17.f * ux * rcp32(modu);
     return -(K1 * P.Q * (O - P.OC) * fmaxf(sqrtf(O) - P.sqrt_OC, 0.f));
 }
 
@@ -158,7 +168,7 @@ __device__ __forceinline__ void edge32(const Phys32 &P, const Face32 &a, float u
     const float s0 = sqrtf(h0), s1 = sqrtf(h1);
     const float hm = 0.5f * (h0 + h1);
     const float ss = s0 + s1;
-    const float um = (ss > 0.f) ? (s0 * u0 + s1 * u1) * __frcp_rn(ss) : CUDART_NAN_F;
+    const float um = (ss > 0.f) ? (s0 * u0 + s1 * u1) * rcp32(ss) : CUDART_NAN_F;
     const float sg = 3.1320919526731650f;  // sqrt(9.81)
     float SL = u0 - sg * s0, SR = u1 + sg * s1;
     const float cm = sqrtf(kGf * hm);
@@ -167,7 +177,7 @@ __device__ __forceinline__ void edge32(const Phys32 &P, const Face32 &a, float u
     float a0, a1;
     const float dS = SR - SL;
     if (dS > 1e-30f) {
-        const float r = __frcp_rn(dS);
+        const float r = rcp32(dS);
         a0 = (SR * fabsf(SL) - SL * fabsf(SR)) * r;
         a1 = (fabsf(SR) - fabsf(SL)) * r;
     } else {

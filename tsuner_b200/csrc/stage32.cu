@@ -247,7 +247,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         const float hs = zz + (P.eta0f + HH);  // FP32 when clearly wet, FP64 near dryness
         const float h = (hs > kWetMarginf) ? hs : (float)depth64(zz, HH, eta0);
         float ux, uy, m;
-        const float rh = (h > 0.f) ? __frcp_rn(h) : 0.f;
+        const float rh = (h > 0.f) ? rcp32(h) : 0.f;
         velocity32r(h, rh, sV[2 * PS + idx], sV[3 * PS + idx], ux, uy, m);
         sV[5 * PS + idx] = h;
         sV[6 * PS + idx] = ux;
@@ -513,16 +513,16 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
            // this stage's input, whose depth phase 2 already formed)
             const float h0 = FIRST ? hcell : (float)depth64(v0[0], v0[1], eta0);
             float ux, uy, modu;
-            const float r0 = (h0 > 0.f) ? __frcp_rn(h0) : 0.f;
+            const float r0 = (h0 > 0.f) ? rcp32(h0) : 0.f;
             velocity32r(h0, r0, v0[2], v0[3], ux, uy, modu);
             const float cf = (h0 > 0.f) ? dt * P.FR * modu * r0 : 0.f;
-            const float rf = __frcp_rn(1.f + cf);
+            const float rf = rcp32(1.f + cf);
             qx *= rf;
             qy *= rf;
-            const float c = (h0 + P.eps_h > 0.f) ? v0[4] * __frcp_rn(h0 + P.eps_h) : 0.f;
+            const float c = (h0 + P.eps_h > 0.f) ? v0[4] * rcp32(h0 + P.eps_h) : 0.f;
             const float Z = P.A_er * modu * P.sqrt_FR * P.inv_vs;
             const float Z5 = Z * Z * Z * Z * Z;
-            float Fe = P.VP * (1.3e-7f * Z5) * __frcp_rn(1.f + 4.3e-7f * Z5);
+            float Fe = P.VP * (1.3e-7f * Z5) * rcp32(1.f + 4.3e-7f * Z5);
             Fe = fminf(fmaxf(Fe, 0.f), 0.1f);
             float Fd = fminf(fmaxf(P.vs * P.K_dep * c, 0.f), 0.1f);
             const float phi = (Fe - Fd) * (float)P.suspension;
@@ -558,7 +558,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         } else {
             h = (float)hd;
             float m;
-            const float rh = __frcp_rn(h);  // h > 0 here
+            const float rh = rcp32(h);  // h > 0 here
             velocity32r(h, rh, qx, qy, uxf, uyf, m);
             const float c = fmaxf(hc * rh, 0.f);
             qx = h * uxf;
