@@ -853,12 +853,11 @@ const Variant32 *variants32(int *n) {
     return v;
 }
 
-// single-grid variant: TSU_TILE32 = index into variants32; default 16x16
+// single-grid variant: TSU_TILE32 = index into variants32; default 32x8
 // with 4 resident CTAs per SM (measured fastest at 4096^2: 32 warps per SM
 // hide the fixed-latency dependencies of the flux arithmetic, 16 warps did
-// not; 16x16 has a smaller face/edge fringe than 32x8, 7357 vs 7320
-// Mcell-steps/s)
-constexpr int kSingleDefault = 8;
+// not; 32x8 8579 vs 16x16 8429 Mcell-steps/s with the current code)
+constexpr int kSingleDefault = 6;
 int single_variant() {
     static int k = [] {
         int n;
