@@ -51,22 +51,23 @@ __device__ __forceinline__ int wrap_clamp32(int g, int n, bool periodic) {
     return g < 0 ? 0 : (g >= n ? n - 1 : g);
 }
 
-__device__ __forceinline__ void put_face(float *base, int stride, const Face32 &f) {
-    base[0] = f.h;
-    base[stride] = f.z;
-    base[2 * stride] = f.u;
-    base[3 * stride] = f.v;
-    base[4 * stride] = f.H;
-    base[5 * stride] = f.c;
+// A face in shared memory: three planes of pairs (h, z), (u, v), (H, c),
+// `stride` pairs apart; 8-byte accesses, consecutive items in consecutive
+// pairs (no bank conflicts).
+__device__ __forceinline__ void put_face(float2 *base, int stride, const Face32 &f) {
+    base[0] = make_float2(f.h, f.z);
+    base[stride] = make_float2(f.u, f.v);
+    base[2 * stride] = make_float2(f.H, f.c);
 }
-__device__ __forceinline__ Face32 get_face(const float *base, int stride) {
+__device__ __forceinline__ Face32 get_face(const float2 *base, int stride) {
     Face32 f;
-    f.h = base[0];
-    f.z = base[stride];
-    f.u = base[2 * stride];
-    f.v = base[3 * stride];
-    f.H = base[4 * stride];
-    f.c = base[5 * stride];
+    const float2 a = base[0], b = base[stride], c = base[2 * stride];
+    f.h = a.x;
+    f.z = a.y;
+    f.u = b.x;
+    f.v = b.y;
+    f.H = c.x;
+    f.c = c.y;
     return f;
 }
 
@@ -140,6 +141,9 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     float *sFlux = smem32;
     float *sFx = smem32 + T::kRegA;
     float *sFy = sFx + T::kFx;
+    // faces: [2 sides][3 pair planes][rows][columns] of float2
+    float2 *sFx2 = reinterpret_cast<float2 *>(sFx), *sFy2 = reinterpret_cast<float2 *>(sFy);
+    static_assert(T::kRegA % 2 == 0 && T::kFx % 2 == 0, "8-byte aligned face planes");
     float *sDeta = sFy + T::kFy;
     double *sRed = reinterpret_cast<double *>(sDeta + T::kDeta);  // [3][kWarps]
     unsigned char *sM = reinterpret_cast<unsigned char *>(smem32) + T::kMaskOff;
@@ -284,17 +288,17 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         }
         const int c = (ly + 2) * LX + (lx + HX);
         const int step = xdir ? 1 : LX;
-        float *dst;
+        float2 *dst;
         int fstride, side, didx = -1;
         if (xdir) {
-            dst = sFx + ly * FXW + (lx + 1);
+            dst = sFx2 + ly * FXW + (lx + 1);
             fstride = TY * FXW;
-            side = 6 * TY * FXW;
+            side = 3 * TY * FXW;
             if (k == 0) didx = ty * TX + tx;
         } else {
-            dst = sFy + (ly + 1) * TX + lx;
+            dst = sFy2 + (ly + 1) * TX + lx;
             fstride = FYH * TX;
-            side = 6 * FYH * TX;
+            side = 3 * FYH * TX;
             if (k == 1) didx = TY * TX + ty * TX + tx;
         }
         Face32 fm, fp;
@@ -359,14 +363,14 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         float *outM = nullptr, *outP = nullptr;
         if (inner) {  // interior edges only (uniform per tile): no bounds or boundary cases
             if (vert) {
-                a = get_face(sFx + (6 * TY + r) * FXW + e, TY * FXW);
-                b = get_face(sFx + r * FXW + (e + 1), TY * FXW);
+                a = get_face(sFx2 + (3 * TY + r) * FXW + e, TY * FXW);
+                b = get_face(sFx2 + r * FXW + (e + 1), TY * FXW);
                 fixed = (int)sM[(r + 2) * MLX + e + MHX - 1] * (int)sM[(r + 2) * MLX + e + MHX];
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
                 if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             } else {
-                a = get_face(sFy + (6 * FYH + e) * TX + c, FYH * TX);
-                b = get_face(sFy + (e + 1) * TX + c, FYH * TX);
+                a = get_face(sFy2 + (3 * FYH + e) * TX + c, FYH * TX);
+                b = get_face(sFy2 + (e + 1) * TX + c, FYH * TX);
                 fixed = (int)sM[(e + 1) * MLX + c + MHX] * (int)sM[(e + 2) * MLX + c + MHX];
                 if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
                 if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
@@ -375,8 +379,8 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             const int ex = x0 + e, ey = y0 + r;
             if (ey >= npy || ex > npx) continue;
             const int ly = r + 2;
-            const float *Rf = sFx + (6 * TY + r) * FXW + e;
-            const float *Lf = sFx + r * FXW + (e + 1);
+            const float2 *Rf = sFx2 + (3 * TY + r) * FXW + e;
+            const float2 *Lf = sFx2 + r * FXW + (e + 1);
             if (periodic && (ex == 0 || ex == npx)) {
                 a = get_face(Rf, TY * FXW);
                 b = get_face(Lf, TY * FXW);
@@ -408,8 +412,8 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         } else {
             const int ex = x0 + c, ey = y0 + e;
             if (ex >= npx || ey > npy) continue;
-            const float *Uf = sFy + (6 * FYH + e) * TX + c;
-            const float *Df = sFy + (e + 1) * TX + c;
+            const float2 *Uf = sFy2 + (3 * FYH + e) * TX + c;
+            const float2 *Df = sFy2 + (e + 1) * TX + c;
             if (periodic && (ey == 0 || ey == npy)) {
                 a = get_face(Uf, FYH * TX);
                 b = get_face(Df, FYH * TX);
