@@ -138,7 +138,10 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     float *smem32 = smem_align<128>(smem_raw);
     __shared__ uint64_t sBar;  // the tile's TMA load
     float *sV = smem32;
-    float *sFlux = smem32;
+    // edge fluxes per cell side (4 directions): (f0, f1) and (f2, f3) as
+    // float2 planes, f4 as a float plane; aliases the cell planes (dead by then)
+    float2 *sFA = reinterpret_cast<float2 *>(smem32);  // [2][4][TY * TX]
+    float *sFS = smem32 + 16 * TY * TX;                 // [4][TY * TX]
     float *sFx = smem32 + T::kRegA;
     float *sFy = sFx + T::kFx;
     // faces: [2 sides][3 pair planes][rows][columns] of float2
@@ -360,20 +363,20 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             e = 0;
             c = tid - TY;
         }
-        float *outM = nullptr, *outP = nullptr;
+        int outM = -1, outP = -1;  // flux slots: direction * FS + cell
         if (inner) {  // interior edges only (uniform per tile): no bounds or boundary cases
             if (vert) {
                 a = get_face(sFx2 + (3 * TY + r) * FXW + e, TY * FXW);
                 b = get_face(sFx2 + r * FXW + (e + 1), TY * FXW);
                 fixed = (int)sM[(r + 2) * MLX + e + MHX - 1] * (int)sM[(r + 2) * MLX + e + MHX];
-                if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
-                if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
+                if (e >= 1) outM = 1 * FS + r * TX + (e - 1);
+                if (e < TX) outP = 0 * FS + r * TX + e;
             } else {
                 a = get_face(sFy2 + (3 * FYH + e) * TX + c, FYH * TX);
                 b = get_face(sFy2 + (e + 1) * TX + c, FYH * TX);
                 fixed = (int)sM[(e + 1) * MLX + c + MHX] * (int)sM[(e + 2) * MLX + c + MHX];
-                if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
-                if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
+                if (e >= 1) outM = 3 * FS + (e - 1) * TX + c;
+                if (e < TY) outP = 2 * FS + e * TX + c;
             }
         } else if (vert) {
             const int ex = x0 + e, ey = y0 + r;
@@ -387,27 +390,27 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
                 fixed = sM[ly * MLX + e + MHX - 1];
                 seam = true;
                 seg = npx + ey;
-                if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
-                if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
+                if (e >= 1) outM = 1 * FS + r * TX + (e - 1);
+                if (e < TX) outP = 0 * FS + r * TX + e;
             } else if (ex == 0) {
                 a = get_face(Lf, TY * FXW);
                 sgnn = -1;
                 fixed = sM[ly * MLX + e + MHX];
                 bnd = true;
                 seg = 2 * npx + npy + ey;
-                outM = sFlux + 0 * 5 * FS + r * TX + e;
+                outM = 0 * FS + r * TX + e;
             } else if (ex == npx) {
                 a = get_face(Rf, TY * FXW);
                 fixed = sM[ly * MLX + e + MHX - 1];
                 bnd = true;
                 seg = npx + ey;
-                outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
+                outM = 1 * FS + r * TX + (e - 1);
             } else {
                 a = get_face(Rf, TY * FXW);
                 b = get_face(Lf, TY * FXW);
                 fixed = (int)sM[ly * MLX + e + MHX - 1] * (int)sM[ly * MLX + e + MHX];
-                if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
-                if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
+                if (e >= 1) outM = 1 * FS + r * TX + (e - 1);
+                if (e < TX) outP = 0 * FS + r * TX + e;
             }
         } else {
             const int ex = x0 + c, ey = y0 + e;
@@ -420,27 +423,27 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
                 fixed = sM[(e + 1) * MLX + c + MHX];
                 seam = true;
                 seg = npx + npy + ex;
-                if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
-                if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
+                if (e >= 1) outM = 3 * FS + (e - 1) * TX + c;
+                if (e < TY) outP = 2 * FS + e * TX + c;
             } else if (ey == 0) {
                 a = get_face(Df, FYH * TX);
                 sgnn = -1;
                 fixed = sM[(e + 2) * MLX + c + MHX];
                 bnd = true;
                 seg = ex;
-                outM = sFlux + 2 * 5 * FS + e * TX + c;
+                outM = 2 * FS + e * TX + c;
             } else if (ey == npy) {
                 a = get_face(Uf, FYH * TX);
                 fixed = sM[(e + 1) * MLX + c + MHX];
                 bnd = true;
                 seg = npx + npy + ex;
-                outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
+                outM = 3 * FS + (e - 1) * TX + c;
             } else {
                 a = get_face(Uf, FYH * TX);
                 b = get_face(Df, FYH * TX);
                 fixed = (int)sM[(e + 1) * MLX + c + MHX] * (int)sM[(e + 2) * MLX + c + MHX];
-                if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
-                if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
+                if (e >= 1) outM = 3 * FS + (e - 1) * TX + c;
+                if (e < TY) outP = 2 * FS + e * TX + c;
             }
         }
         if (bnd) {
@@ -478,19 +481,15 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         const float m2 = vert ? sgnn * Dm[2] : sgnn * Dm[1];
         const float p1 = vert ? sgnn * Dp[1] : -sgnn * Dp[2];
         const float p2 = vert ? sgnn * Dp[2] : sgnn * Dp[1];
-        if (outM) {
-            outM[0] = Dm[0];
-            outM[FS] = m1;
-            outM[2 * FS] = m2;
-            outM[3 * FS] = Dm[3];
-            outM[4 * FS] = Dm[4];
+        if (outM >= 0) {
+            sFA[outM] = make_float2(Dm[0], m1);
+            sFA[4 * FS + outM] = make_float2(m2, Dm[3]);
+            sFS[outM] = Dm[4];
         }
-        if (outP) {
-            outP[0] = Dp[0];
-            outP[FS] = p1;
-            outP[2 * FS] = p2;
-            outP[3 * FS] = Dp[3];
-            outP[4 * FS] = Dp[4];
+        if (outP >= 0) {
+            sFA[outP] = make_float2(Dp[0], p1);
+            sFA[4 * FS + outP] = make_float2(p2, Dp[3]);
+            sFS[outP] = Dp[4];
         }
     }
     __syncthreads();
@@ -536,11 +535,20 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
         }
         const float invx = dt * P.inv_dx, invy = dt * P.inv_dy;
         const int cell = ty * TX + tx;
+        float fl[4][5];  // the four sides' fluxes of this cell
+#pragma unroll
+        for (int d = 0; d < 4; d++) {
+            const float2 a = sFA[d * FS + cell], b = sFA[(4 + d) * FS + cell];
+            fl[d][0] = a.x;
+            fl[d][1] = a.y;
+            fl[d][2] = b.x;
+            fl[d][3] = b.y;
+            fl[d][4] = sFS[d * FS + cell];
+        }
         float dv[5];
 #pragma unroll
         for (int f = 0; f < 5; f++)
-            dv[f] = invx * (sFlux[(0 * 5 + f) * FS + cell] + sFlux[(1 * 5 + f) * FS + cell]) +
-                    invy * (sFlux[(2 * 5 + f) * FS + cell] + sFlux[(3 * 5 + f) * FS + cell]);
+            dv[f] = invx * (fl[0][f] + fl[1][f]) + invy * (fl[2][f] + fl[3][f]);
         z -= dv[0] - dv[3];
         qx -= dv[1];
         qy -= dv[2];
