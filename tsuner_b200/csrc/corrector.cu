@@ -436,7 +436,9 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
 #pragma unroll
         for (int q = 0; q < 4; q++) tma_load_4d(stg + kWgPatchBuf + q * kZPlane, &tmZ, 8 * q, x0, y0, img, &full[st]);
     };
-    int last_load = -1, last_mma = -1;  // iterations whose load / MMAs tid 0 issued (for the error path)
+    // for the error path (tid 0): the last iteration whose load was issued, the
+    // last whose load was waited for, and the last whose MMAs were committed
+    int last_load = -1, consumed = -1, last_mma = -1;
     if (tid == 0 && (int)blockIdx.x < G.total) {
         issue(blockIdx.x, 0);
         last_load = 0;
@@ -466,6 +468,7 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
             failed = true;
             break;
         }
+        consumed = i;
         if (tid == 0) {
             // D[dy * 32 + cin (+ 32 ignored rows)][cout] for each dx: A = the
             // shifted patch (M groups (dy, quarter) 160 B apart, K groups =
@@ -506,7 +509,9 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
         if (tid == 0) {
             atomicExch(&g_corr_err, 1);
             // whatever may still run: the last load and the last MMAs
-            if (last_load >= 0) mbar_wait(&full[last_load & 1], (last_load >> 1) & 1);
+            // loads issued but not waited for (up to two: this tile's and the next)
+            for (int k = consumed + 1; k <= last_load; k++) mbar_wait(&full[k & 1], (k >> 1) & 1);
+            // the last commit covers every earlier MMA of this thread
             if (last_mma >= 0) mbar_wait(&done[last_mma & 1], (last_mma >> 1) & 1);
         }
     } else if (n > 0) {
