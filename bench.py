@@ -347,7 +347,7 @@ def run_corrector(a, rank, world, local, dist):
         "ms_per_step": round(ms_conv, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "bf16 (fp32 accumulate)", "data": "synthetic (seeded site and sources, solver-generated pairs)",
         "config": {"workload": "corrector: fine %dx%d dx=%.0fm <- coarse %dx%d, %d train pairs (FP32 ensembles), "
-                               "%d held-out sources judged against the FP64 plain solve, t_end %.0f s"
+                               "%d held-out sources compared against the FP64 plain solve, t_end %.0f s"
                                % (n, n, site.dx, n // f, n // f, len(train_src), len(test_src), t_end),
                    "network": "6 x conv3x3 32 ch, BF16 weights/activations, FP32 accumulate (tcgen05, TMEM)",
                    "train": {"iters": a.corr_iters, "batch": 8, "lr": "1e-3 / 3e-4 / 1e-4 (1/2, 1/4, 1/4 of the steps)",

@@ -1,6 +1,6 @@
 """GPU tests of the FP32 precision form (TsuSwitches.precision = 1).
 
-It has no reference counterpart, so it is judged against the FP64 plain form
+It has no reference counterpart, so it is compared against the FP64 plain form
 (itself value-identical to the reference kernels):
   * lake at rest is preserved exactly (z = eta - eta0 == 0, q == 0) over a
     rough bed with a raised sea level -- the property FP32 loses without the
