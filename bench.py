@@ -3,7 +3,7 @@
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload nwave4096|nwave2048|hump512|humps8192|ensembleN|corrector]
-                  [--no-cpu-baseline]
+                  [--precision fp64|fp32] [--no-cpu-baseline] [--no-config3]
 
 One "step" is one full time step of the scheme (2 RK stages: MUSCL faces,
 edge fluxes with bedload, volume update, running extrema, CFL dt) over the
@@ -11,12 +11,19 @@ whole grid.  Default workload: the 4096^2 shelf with the west N-wave
 (seeded synthetic inputs, no dataset).  The state (671 MB in FP64) is far
 larger than the 126 MB L2, so no L2 flush is needed between steps.
 
---impl ours       the product library (libtsuner_b200.so) through its C ABI
+--impl ours       the product library (libtsuner_b200.so) through its C ABI.
+                  The line's `value` / `e2e` are the FP64 plain form -- the
+                  reference's own arithmetic, value-identical to its kernels;
+                  the FP32 precision form rides along (`fp32_form`,
+                  `fp32_vs_fp64`), and at one GPU the 8192^2 humps
+                  configuration runs both forms for a fixed 2000 steps
+                  (`config3`: rates, roofline, L-inf / L2 / mass drift).
 --impl reference  the reference's own CUDA kernels, unmodified, built by
                   oracle/build_ref.py and driven step by step on the same GPU
                   and inputs (the reference has no CPU implementation of the
                   path); without a GPU or without oracle/_ref it falls back to
-                  the oracle port on the host cores.
+                  the oracle port on the host cores.  It never loads the
+                  product library.
 
 Multi-GPU (torchrun, one rank per GPU): every rank advances its own replica
 (weak scaling, no data-path collective); the reported time is the max over
@@ -43,6 +50,13 @@ METRIC = "Mcell-steps/s: FP32 fused vs FP64 plain at stated L-inf error; % HBM p
 # (5 x 5 planes x element size), mask read twice (2 x 1 B), hmax/bmin/eta_max
 # read-modify-write (3 x 2 x element size)
 BYTES_PER_CELL_STEP = {"f64": 5 * 5 * 8 + 2 + 3 * 16, "f32": 5 * 5 * 4 + 2 + 3 * 8}
+# the arithmetic both arms compute (the reference's scheme, FP64)
+SCHEME = ("FP64; order 2 MUSCL + RK2, HLL-type edge fluctuations with the Ashida-Michiue bedload, Chezy friction, "
+          "erosion/deposition, running extrema and the CFL dt every step")
+FORM = {0: "fp64 plain form (value-identical to the reference kernels); one fused kernel per RK stage",
+        1: "fp32 precision form (FP32 state, FP64 still-water level / wet-dry reconstruction / sums / time); "
+           "one fused kernel per RK stage"}
+CONFIG3_SIDE = 8192
 
 
 def peaks():
@@ -65,6 +79,13 @@ def workload(name):
     if name == "humps8192":
         return W.humps_shelf(8192, 8192, 5.0), "humps_shelf 8192x8192 dx=5m (8 seeded humps, walls)"
     raise SystemExit("unknown workload " + name)
+
+
+def arm_config(desc, n, world):
+    """The config dict both arms print (identical apart from `impl`)."""
+    return {"workload": desc, "cells": n, "scheme": SCHEME,
+            "l2": "FP64 state %.0f MB > 126 MB L2, no flush needed" % (5 * 8 * n / 1e6),
+            "parallelism": "replicas x%d" % world}
 
 
 class Clocks:
@@ -184,36 +205,35 @@ def cpu_baseline(max_seconds=20.0):
 
 
 def traffic_from_profiles(name):
-    """Per-launch DRAM bytes of the stage kernels recorded by ncu (profiles/)."""
+    """Per-cell-step DRAM bytes of the stage kernels recorded by ncu (profiles/
+    traffic.txt): (bytes per cell-step, cells of the capture, capture it came
+    from -- another workload's name when the row is scaled per cell)."""
     path = os.path.join(ROOT, "profiles", "traffic.txt")
     try:
         for line in open(path):
             parts = line.split()
-            if len(parts) >= 3 and parts[0] == name:
-                return float(parts[1]), float(parts[2])  # bytes per cell-step, cells of the capture
+            if len(parts) >= 4 and parts[0] == name:
+                return float(parts[1]), float(parts[2]), parts[3]
     except OSError:
         pass
     return None
 
 
-def timed_form(T, w, sw, a, local, dist):
-    """W warm-up steps, then K device-timed steps (CUDA events on the solver's
-    stream, barrier + sync on both sides).  Returns the solver (state after
-    W + K steps) and the timing."""
-    s = T.Solver(w.p, sw, device=local)
-    s.set_state(w.V)
-    s.set_mask(w.mask)
-    if sw.read_files:
-        s.set_boundary_series(w.CC, w.tCC)
-    s.reset()
-    s.step(a.warmup)
-    s.sync()
-    barrier(dist, local)
-    with Clocks(local) as clk:
-        s.step(a.steps)
-        s.sync()
-    ms = s.last_ms()
-    return s, ms, s.last_launches(), clk.summary()
+def roofline(form, n, steps, ms, tr_key=None):
+    hbm, kind = peaks()
+    bpc = BYTES_PER_CELL_STEP[form]
+    achieved = bpc * n * steps / (ms / 1e3) / 1e9
+    r = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+         "peak_kind": kind, "bytes_per_cell_step": bpc, "traffic": None,
+         "note": "algorithmic bytes per cell-step x cells x steps / device time of the stage kernels "
+                 "(CUDA events on the solver stream); the kernel is bound by instruction issue, not HBM"}
+    tr = traffic_from_profiles(tr_key) if tr_key else None
+    if tr is not None:
+        # per launch, like `achieved`: bytes per cell-step x cells / 2 stage launches
+        r["traffic"] = round(tr[0] * n / 2.0, 0)
+        r["traffic_source"] = ("ncu dram__bytes_read+write of this workload" if tr[2] == tr_key else
+                               "ncu dram__bytes of the %s capture (%.0f cells) scaled per cell" % (tr[2], tr[1]))
+    return r
 
 
 def form_switches(w, precision):
@@ -222,6 +242,102 @@ def form_switches(w, precision):
     return make_switches(order=sw.order, wbc=sw.wbc, bedload=sw.bedload, suspension=sw.suspension,
                          read_files=sw.read_files, bedload_law=sw.bedload_law, precision=precision,
                          grass_ag=sw.grass_ag, eta0=sw.eta0)
+
+
+def load_solver(T, w, sw, local):
+    s = T.Solver(w.p, sw, device=local)
+    s.set_state(w.V)
+    s.set_mask(w.mask)
+    if sw.read_files:
+        s.set_boundary_series(w.CC, w.tCC)
+    s.reset()
+    return s
+
+
+def run_form(T, w, prec, warmup, steps, local, dist, e2e=True):
+    """W warm-up steps, then K device-timed steps (CUDA events on the solver's
+    stream, barrier + sync on both sides); then, if e2e, the same K steps end
+    to end through the C ABI with host buffers (upload, reset, K steps, state
+    and extrema read back).  Returns the state after W + K steps and the
+    timings."""
+    sw = form_switches(w, prec)
+    s = load_solver(T, w, sw, local)
+    s.step(warmup)
+    s.sync()
+    barrier(dist, local)
+    with Clocks(local) as clk:
+        s.step(steps)
+        s.sync()
+    out = {"ms": dist_max(dist, s.last_ms(), local), "ms_local": s.last_ms(), "launches": s.last_launches(),
+           "clocks": clk.summary(), "V": s.state(), "sums": s.sums() if prec == 1 else None}
+    if e2e:
+        barrier(dist, local)
+        t0 = time.perf_counter()
+        s.set_state(w.V)
+        s.set_mask(w.mask)
+        if sw.read_files:
+            s.set_boundary_series(w.CC, w.tCC)
+        s.reset()
+        s.step(steps)
+        Vout = s.state()
+        s.extrema()
+        out["e2e_s"] = dist_max(dist, time.perf_counter() - t0, local)
+        assert np.isfinite(Vout).all()
+    s.close()
+    return out
+
+
+def e2e_line(world, n, steps, e2e_s, w):
+    h2d = 5 * 8 * n + 4 * n + (w.CC.nbytes + w.tCC.nbytes if w.sw.read_files else 0)
+    d2h = 5 * 8 * n + 3 * 8 * n
+    return {"value": round(world * n * steps / e2e_s / 1e6, 3), "unit": "Mcell-steps/s",
+            "h2d_bytes_per_step": int(h2d / steps), "d2h_bytes_per_step": int(d2h / steps),
+            "what": "tsu_set_state/mask/series + tsu_reset + tsu_step(K) + tsu_get_state/extrema, host buffers "
+                    "(copies inside the timed region, amortised over the K = %d steps)" % steps}
+
+
+def depth_errors(V32, V64, eps_h):
+    wet = V64[0] > eps_h
+    dh = V32[0] - V64[0]
+    m32, m64 = float(V32[0].sum()), float(V64[0].sum())
+    return {"linf_depth_m": float(np.abs(dh).max()),
+            "l2_depth_m": float(np.sqrt(np.mean(dh[wet] ** 2))) if wet.any() else 0.0,
+            "linf_qx": float(np.abs(V32[1] - V64[1]).max()),
+            "linf_bed_m": float(np.abs(V32[3] - V64[3]).max()),
+            "mass_drift_rel": (m32 - m64) / m64 if m64 else None}
+
+
+def run_config3(a, T, local):
+    """Config 3: humps_shelf 8192^2 (67.1 M cells), both forms for a fixed
+    number of steps from the same initial state (5 untimed, the rest timed),
+    then the FP32 form's depth error and mass drift against the FP64 form."""
+    from tsuner_b200 import workloads as W
+    w = W.humps_shelf(CONFIG3_SIDE, CONFIG3_SIDE, 5.0)
+    n = w.ncells
+    total, warm = a.config3_steps, 5
+    timed = total - warm
+    m0 = float(w.V[0].sum())
+    r = {}
+    for prec in (1, 0):
+        r[prec] = run_form(T, w, prec, warm, timed, local, None, e2e=False)
+    V32, V64 = r[1]["V"], r[0]["V"]
+    err = depth_errors(V32, V64, w.p.epsilon_h)
+    err["steps"] = total
+    err["mass_change_rel"] = {"fp32": (float(V32[0].sum()) - m0) / m0, "fp64": (float(V64[0].sum()) - m0) / m0}
+    err["bound_linf_depth_m"] = 1e-4
+    out = {"workload": "humps_shelf %dx%d dx=5m (8 seeded humps 0.5-4 m / sigma 200-2000 m, fractal shelf, "
+                       "harbour mask, walls), %d steps (%d warm-up + %d timed)" % (CONFIG3_SIDE, CONFIG3_SIDE, total,
+                                                                              warm, timed),
+           "cells": n}
+    for prec, key, form in ((1, "fp32", "f32"), (0, "fp64", "f64")):
+        out[key] = {"value": round(n * timed / (r[prec]["ms"] / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
+                    "ms_per_step": round(r[prec]["ms"] / timed, 4),
+                    "roofline": roofline(form, n, timed, r[prec]["ms"],
+                                         ("stage32_" if prec else "stage64_") + "humps8192"),
+                    "clocks": r[prec]["clocks"], "gpu_launches": r[prec]["launches"]}
+    out["fp32_over_fp64"] = round(r[0]["ms"] / r[1]["ms"], 3)
+    out["fp32_vs_fp64"] = err
+    return out
 
 
 def run_ensemble(a, rank, world, local, dist):
@@ -374,121 +490,97 @@ def run_ours(a, rank, world, local, dist):
     w, desc = workload(a.workload)
     n = w.ncells
     prim = 1 if a.precision == "fp32" else 0
-    # ---- primary form, device-timed with inputs resident in HBM
-    s, ms, launches, clocks = timed_form(T, w, form_switches(w, prim), a, local, dist)
-    ms_max = dist_max(dist, ms, local)
-    V_prim = s.state()
-    sums = s.sums() if prim == 1 else None
-    # ---- end to end through the C ABI with host buffers
-    barrier(dist, local)
-    t0 = time.perf_counter()
-    s.set_state(w.V)
-    s.set_mask(w.mask)
-    if w.sw.read_files:
-        s.set_boundary_series(w.CC, w.tCC)
-    s.reset()
-    s.step(a.steps)
-    Vout = s.state()
-    s.extrema()
-    e2e_s = dist_max(dist, time.perf_counter() - t0, local)
-    s.close()
-    assert np.isfinite(Vout).all()
-    # ---- the other form on the same workload and step count (rate + error)
-    other = None
-    if prim == 1 and not a.no_fp64:
-        s64, ms64, _, _ = timed_form(T, w, form_switches(w, 0), a, local, dist)
-        ms64 = dist_max(dist, ms64, local)
-        V64 = s64.state()
-        s64.close()
-        wet = V64[0] > w.p.epsilon_h
-        dh = V_prim[0] - V64[0]
-        m64 = float(V64[0].sum())
-        hbm64, kind64 = peaks()
-        ach64 = BYTES_PER_CELL_STEP["f64"] * n * a.steps / (ms64 / 1e3) / 1e9
-        other = {"fp64_plain": {"value": round(world * n * a.steps / (ms64 / 1e3) / 1e6, 3),
-                                "unit": "Mcell-steps/s", "ms_per_step": round(ms64 / a.steps, 4),
-                                "roofline": {"bound": "hbm", "achieved": round(ach64, 1), "peak": hbm64,
-                                             "unit": "GB/s", "frac": round(ach64 / hbm64, 4), "peak_kind": kind64,
-                                             "bytes_per_cell_step": BYTES_PER_CELL_STEP["f64"]}},
-                 "fp32_vs_fp64": {"steps": a.warmup + a.steps,
-                                  "linf_depth_m": float(np.abs(dh).max()),
-                                  "l2_depth_m": float(np.sqrt(np.mean(dh[wet] ** 2))) if wet.any() else 0.0,
-                                  "linf_qx": float(np.abs(V_prim[1] - V64[1]).max()),
-                                  "mass_drift_rel": (sums[0] - m64) / m64 if sums else None,
-                                  "speedup": round(ms64 / ms, 3)}}
-    h2d = 5 * 8 * n + 4 * n + (w.CC.nbytes + w.tCC.nbytes if w.sw.read_files else 0)
-    d2h = 5 * 8 * n + 3 * 8 * n
+    other = 1 - prim
+    # ---- primary form: device-timed with inputs resident in HBM, then end to end
+    P = run_form(T, w, prim, a.warmup, a.steps, local, dist)
+    # ---- the other form on the same workload and step count (rate, e2e, error)
+    O = None if a.no_other else run_form(T, w, other, a.warmup, a.steps, local, dist)
+    C3 = None
+    if world == 1 and not a.no_config3 and a.workload == "nwave4096":
+        C3 = run_config3(a, T, local)
     if rank != 0:
         return None
-    value = world * n * a.steps / (ms_max / 1e3) / 1e6
-    hbm, kind = peaks()
     dtype = "f32" if prim == 1 else "f64"
-    bpc = BYTES_PER_CELL_STEP[dtype]
-    achieved = bpc * n * a.steps / (ms / 1e3) / 1e9
-    tr = traffic_from_profiles(("stage32_" if prim else "stage64_") + a.workload)
-    form = ("fp32 precision form (FP32 state, FP64 still-water level / wet-dry reconstruction / sums / time)"
-            if prim else "fp64 plain form (value-identical to the reference kernels)")
     line = {
-        "metric": METRIC, "value": round(value, 3), "unit": "Mcell-steps/s", "n_gpus": world,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 4),
+        "metric": METRIC, "value": round(world * n * a.steps / (P["ms"] / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
+        "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(P["ms"] / a.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
         "data": "synthetic (seeded generators, no dataset)",
-        "config": {"workload": desc, "form": form + "; one fused kernel per RK stage",
-                   "cells": n, "l2": "state %.0f MB > 126 MB L2, no flush needed" % (5 * (4 if prim else 8) * n / 1e6),
-                   "parallelism": "replicas x%d" % world},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                     "frac": round(achieved / hbm, 4), "peak_kind": kind,
-                     "bytes_per_cell_step": bpc,
-                     "traffic": None if tr is None else round(tr[0] * n / 2.0, 0),
-                     "note": "algorithmic bytes per cell-step x cells x steps / device time of the stage kernels"},
-        "gpu_launches": launches,
-        "e2e": {"value": round(world * n * a.steps / e2e_s / 1e6, 3), "unit": "Mcell-steps/s",
-                "h2d_bytes_per_step": int(h2d / a.steps), "d2h_bytes_per_step": int(d2h / a.steps),
-                "what": "tsu_set_state/mask/series + tsu_reset + tsu_step(K) + tsu_get_state/extrema, host buffers"},
-        "clocks": clocks,
+        "config": arm_config(desc, n, world),
+        "form": FORM[prim],
+        "roofline": roofline(dtype, n, a.steps, P["ms_local"], ("stage32_" if prim else "stage64_") + a.workload),
+        "gpu_launches": P["launches"],
+        "e2e": e2e_line(world, n, a.steps, P["e2e_s"], w),
+        "clocks": P["clocks"],
     }
-    if other:
-        line.update(other)
+    if O is not None:
+        key = "fp32_form" if other == 1 else "fp64_plain"
+        oform = "f32" if other == 1 else "f64"
+        line[key] = {"value": round(world * n * a.steps / (O["ms"] / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
+                     "ms_per_step": round(O["ms"] / a.steps, 4), "form": FORM[other],
+                     "roofline": roofline(oform, n, a.steps, O["ms_local"],
+                                          ("stage32_" if other else "stage64_") + a.workload),
+                     "e2e": e2e_line(world, n, a.steps, O["e2e_s"], w), "gpu_launches": O["launches"],
+                     "clocks": O["clocks"]}
+        V32, V64 = (P["V"], O["V"]) if prim == 1 else (O["V"], P["V"])
+        err = depth_errors(V32, V64, w.p.epsilon_h)
+        err["steps"] = a.warmup + a.steps
+        ms32, ms64 = (P["ms"], O["ms"]) if prim == 1 else (O["ms"], P["ms"])
+        err["speedup"] = round(ms64 / ms32, 3)
+        line["fp32_vs_fp64"] = err
+    if C3 is not None:
+        line["config3"] = C3
     if world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
     return line
 
 
 def run_reference(a, rank, world, local, dist):
-    if rank != 0:
-        return None
+    """The reference's own CUDA kernels (oracle/_ref/default: the makefile
+    recipe build of its unmodified GPU sources) on the same workload, one
+    replica per rank; without a GPU or without the build, the oracle port on
+    rank 0's host cores.  The product library is never loaded here."""
     import oracle
     w, desc = workload(a.workload)
     n = w.ncells
-    gpu_ok = False
-    try:
-        import tsuner_b200 as T
-        gpu_ok = T.lib().checkCUDAsupport(local) == 0
-    except Exception:
-        gpu_ok = False
-    if gpu_ok and oracle.ref_available("default"):
+    if n > 53687091:  # GPU/main_TSUNER.cu:60-90: int size arithmetic overflows above this
+        if rank == 0:
+            return {"impl": "reference", "unavailable": "the reference cannot allocate a %dx%d grid (int overflow in "
+                                                         "its size arithmetic, GPU/main_TSUNER.cu:60-90)"
+                                                         % (w.p.npx, w.p.npy)}
+        return None
+    gpu_ok = oracle.ref_gpu_count("default") > local
+    if gpu_ok:
         CC, tCC = (w.CC, w.tCC) if w.sw.read_files else oracle_expired(w)
         oracle.ref_run("default", w.p, w.V, w.mask, CC, tCC, a.warmup, device=local)
+        barrier(dist, local)
         with Clocks(local) as clk:
             t0 = time.perf_counter()
             r = oracle.ref_run("default", w.p, w.V, w.mask, CC, tCC, a.steps, device=local)
             wall = time.perf_counter() - t0
-        value = n * a.steps / (r["ms"] / 1e3) / 1e6
-        return {"metric": METRIC, "value": round(value, 3), "unit": "Mcell-steps/s", "n_gpus": 1,
-                "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(r["ms"] / a.steps, 4),
+        ms = dist_max(dist, r["ms"], local)
+        wall = dist_max(dist, wall, local)
+        if rank != 0:
+            return None
+        value = world * n * a.steps / (ms / 1e3) / 1e6
+        return {"metric": METRIC, "value": round(value, 3), "unit": "Mcell-steps/s", "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded generators, no dataset)", "impl": "reference",
-                "reference_kind": "reference CUDA build (unmodified GPU/*.cu kernels, -O2 -fmad=false -rdc -dlto, sm_100a)",
-                "config": {"workload": desc, "cells": n, "parallelism": "single GPU"},
-                "e2e": {"value": round(n * a.steps / wall / 1e6, 3), "unit": "Mcell-steps/s",
-                        "h2d_bytes_per_step": int((5 * 8 * n + 4 * n) / a.steps),
+                "reference_kind": "reference CUDA build (unmodified GPU/*.cu kernels, -O2 -fmad=false -rdc -dlto, "
+                                  "sm_100a), stepped by oracle/ref_build/ref_harness.cu",
+                "config": arm_config(desc, n, world),
+                "e2e": {"value": round(world * n * a.steps / wall / 1e6, 3), "unit": "Mcell-steps/s",
+                        "h2d_bytes_per_step": int((5 * 8 * n + 4 * n + (CC.nbytes + tCC.nbytes)) / a.steps),
                         "d2h_bytes_per_step": int((5 * 8 * n + 3 * 8 * n) / a.steps),
                         "what": "whole harness call: allocation, upload, K steps, download"},
                 "clocks": clk.summary()}
+    if rank != 0:
+        return None
     cb = cpu_baseline()
     return {"metric": METRIC, "value": cb["value"], "unit": "Mcell-steps/s", "n_gpus": 1, "steps": a.steps,
             "warmup": a.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic", "impl": "reference", "config": {"workload": desc},
+            "dtype": "f64", "data": "synthetic", "impl": "reference", "config": arm_config(desc, n, world),
             "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "Mcell-steps/s",
                                         "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -506,8 +598,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="nwave4096")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="form of the line's value / e2e (the other form is reported beside it)")
+    ap.add_argument("--no-other", "--no-fp64", dest="no_other", action="store_true",
+                    help="skip the other form's run")
+    ap.add_argument("--no-config3", action="store_true", help="skip the 8192^2 configuration")
+    ap.add_argument("--config3-steps", type=int, default=2000, help="steps of the 8192^2 configuration")
     ap.add_argument("--corr-fine", type=int, default=512, help="corrector: fine grid side")
     ap.add_argument("--corr-train", type=int, default=128, help="corrector: training pairs")
     ap.add_argument("--corr-test", type=int, default=16, help="corrector: held-out sources")
@@ -515,6 +611,7 @@ def main():
     ap.add_argument("--corr-tend", type=float, default=600.0, help="corrector: simulated seconds per source")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
+    a.config3_steps = max(a.config3_steps, 10)
     rank, world, local, dist = dist_setup(a.gpus)
     try:
         if a.impl == "reference":

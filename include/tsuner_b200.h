@@ -175,6 +175,14 @@ int tsu_step(TsuSolver *s, long nsteps);
 /* Steps while t < t_end (the reference loop condition), at most max_steps;
  * *steps_done gets the number of steps taken.  Synchronises. */
 int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *steps_done);
+/* Waits for the solver's stream, then reports the kernels' status words:
+ * TSU_ERR_CUDA when a bounded device wait expired (the step it happened in
+ * is unfinished), TSU_ERR_NONFINITE when a cell of the state became NaN or
+ * infinite (checked on the last RK stage of every step and by tsu_reset on
+ * the uploaded state; the reference has no such check and steps on).  After
+ * either, the solver steps again only after tsu_reset (and, for a
+ * non-finite state, a new tsu_set_state).  tsu_get_time and tsu_run_until
+ * report the same words; TSUNER() returns the code. */
 int tsu_sync(TsuSolver *s);
 /* 5*nvol doubles SoA (h, qx, qy, H, hc). */
 int tsu_get_state(TsuSolver *s, double *V);
@@ -264,13 +272,25 @@ int tsu_corr_conv3x3_wgrad(const void *X, const void *dZ, int nimg, int H, int W
 int tsu_corr_status(void);
 const char *tsu_corr_last_error(void);
 
+/* Limit, in nanoseconds, of the kernels' ordinary bounded waits on their own
+ * TMA copies and tensor-core MMAs (stage kernels of every form, corrector
+ * convolutions) on the CURRENT device; 0 restores the default 0.5 s.  No
+ * counterpart in the reference (whose kernels never wait).  It exists so
+ * that the error path can be exercised without a GPU fault: with a limit of
+ * a few nanoseconds the waits expire while the copies are still in flight,
+ * the kernels record the error (tsu_sync / tsu_corr_status report
+ * TSU_ERR_CUDA), drain their own copies and MMAs with the full limit, free
+ * their tensor memory and return, and the context stays usable.  Call it
+ * between steps, with no kernel of the library running. */
+int tsu_set_wait_limit_ns(unsigned long long ns);
+
 /* CFL time step of an FP64 state that the caller already holds in device
  * memory, computed without any device allocation by the library.  No
  * counterpart in the reference (its MinReduction works on a buffer that
  * TSUNER() allocates).  It is for callers that cannot let a library call
  * cudaMalloc: a host framework that owns every device byte through its own
- * pool, code being captured into a CUDA graph (allocation is not allowed
- * there), or a long-running service that forbids allocation after start-up.
+ * pool, or a long-running service that forbids allocation after start-up so
+ * that its memory use stays fixed.
  * d_h, d_qx, d_qy: device planes of p->npy rows, row pitch `pitch_elems`
  * doubles; d_dt: one device double that receives the step, with the same
  * value tsu_reset() computes (GetDeltaT + MinReduction of the reference,
@@ -281,8 +301,11 @@ const char *tsu_corr_last_error(void);
  * exit), so grids above 16384 CTAs of 32 x 8 cells (4,194,304 cells) are
  * rejected with TSU_ERR_INVALID and a message.  The first call on a device
  * looks up the array's device address on that device (make that first call
- * before any stream capture).  Every call shares the array: calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * before any stream capture).  The looked-up address is kept for the life of
+ * the process, so do not call this entry point again on a device after
+ * cudaDeviceReset() there.  Every call shares the array: calls that overlap
+ * on the GPU race and must be serialised by the caller.  Failures leave
+ * their text in tsu_last_error(). */
 int tsu_cfl_dt_noalloc(const double *d_h, const double *d_qx, const double *d_qy, long pitch_elems,
                        const SimParams *p, double *d_dt, void *stream);
 /* Bulk host <-> device copies through the library's pinned staging chunks

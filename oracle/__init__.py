@@ -123,6 +123,22 @@ def ref_lib(variant="default"):
     return _REF[variant]
 
 
+def ref_gpu_count(variant="default"):
+    """CUDA devices visible to the reference build (0 without a GPU or driver);
+    asks the reference library's own CUDA runtime, so the product library is
+    not loaded."""
+    if not ref_available(variant):
+        return 0
+    L = ref_lib(variant)
+    f = getattr(L, "ref_device_count", None) or getattr(L, "cudaGetDeviceCount", None)
+    if f is None:
+        return 0
+    n = C.c_int(0)
+    f.argtypes = [C.POINTER(C.c_int)]
+    f.restype = C.c_int
+    return n.value if f(C.byref(n)) == 0 else 0
+
+
 def ref_switches(variant="default"):
     out = np.zeros(6, np.int32)
     ref_lib(variant).ref_switches(out)

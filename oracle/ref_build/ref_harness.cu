@@ -24,6 +24,19 @@
 
 extern "C" {
 
+/* Number of CUDA devices this build can see (0 on error), so that callers can
+ * probe for a GPU without loading any other library. */
+int ref_device_count(int *n)
+{
+    int k = 0;
+    if (cudaGetDeviceCount(&k) != cudaSuccess) {
+        cudaGetLastError();
+        k = 0;
+    }
+    *n = k;
+    return 0;
+}
+
 /* Compile-time switches of this build (Sim_parameters.hxx values). */
 int ref_switches(int *out6)
 {

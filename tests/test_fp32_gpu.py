@@ -97,6 +97,7 @@ def test_depth_error_vs_fp64(make, steps, bound):
     V64, e64, t64, _ = run(w, sw_of(w, precision=0), steps)
     V32, e32, t32, _ = run(w, sw_of(w, precision=1), steps)
     linf = np.abs(V32[0] - V64[0]).max()
+    print("FP32 vs FP64 L-inf depth after %d steps: %.3e m (bound %.1e)" % (steps, linf, bound))
     assert linf <= bound, linf
     assert abs(t32[0] - t64[0]) / t64[0] < 1e-3
     wet = (e64[0] > -1e29) & (e32[0] > -1e29)
@@ -117,3 +118,32 @@ def test_fp32_switch_variants_follow_fp64(kw):
     assert abs(t - t64) / t64 < 1e-3
     assert np.abs(V[0] - V64[0]).max() <= RUNUP_LINF_M, np.abs(V[0] - V64[0]).max()
     assert np.abs(V[3] - V64[3]).max() <= RUNUP_LINF_M  # bed (Exner) follows too
+
+
+NORTH_STAR_LINF_M = 1e-4  # the stated bar of the FP32 form at the 8192^2 configuration
+
+
+def test_config3_humps8192_2000_steps_within_1e4_m():
+    """The 8192^2 humps configuration as stated (67.1 M cells, 8 seeded humps
+    over the fractal shelf with its wet/dry fronts, harbour mask, walls,
+    2000 steps): the FP32 form's depth stays within 1e-4 m L-inf of the FP64
+    plain form and its water volume within 1e-9 relative of the FP64 form's.
+    L2 over wet cells, the mass drift and each form's change of the water
+    volume since the start are printed."""
+    w = W.humps_shelf(8192, 8192, 5.0)
+    m0 = float(w.V[0].sum())
+    V64, e64, t64, _ = run(w, sw_of(w, precision=0), 2000)
+    V32, e32, t32, sums = run(w, sw_of(w, precision=1), 2000)
+    dh = V32[0] - V64[0]
+    linf = float(np.abs(dh).max())
+    wet = V64[0] > w.p.epsilon_h
+    l2 = float(np.sqrt(np.mean(dh[wet] ** 2)))
+    m32, m64 = float(V32[0].sum()), float(V64[0].sum())
+    drift = (m32 - m64) / m64
+    print("config 3: L-inf %.3e m, L2 %.3e m, mass drift FP32 vs FP64 %.2e, water change FP32 %.2e FP64 %.2e"
+          % (linf, l2, drift, (m32 - m0) / m0, (m64 - m0) / m0))
+    assert t64[2] == t32[2] == 2000
+    assert linf <= NORTH_STAR_LINF_M, linf
+    assert abs(drift) < 1e-9, drift
+    assert abs(sums[0] - m32) / m32 < 1e-12  # the device's FP64 water sum
+    assert abs(t32[0] - t64[0]) / t64[0] < 1e-3

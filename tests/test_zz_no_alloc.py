@@ -1,7 +1,7 @@
 """GPU test of tsu_cfl_dt_noalloc, the CFL-step entry point that allocates
 no device memory (for callers that cannot let a library call cudaMalloc:
-frameworks that own all device memory, code captured into CUDA graphs,
-services that forbid allocation after start-up).
+frameworks that own all device memory through their own pool, services that
+forbid allocation after start-up).
 
 It is called through the C ABI on a state that the ordinary solver holds on
 the device, twice in a row, and each result must equal the step the existing
@@ -51,6 +51,25 @@ def test_noalloc_dt_matches_solver_on_two_calls():
     assert dt0 != dt1
 
 
+def test_noalloc_dt_small_grid_exact_minimum():
+    """At most 4096 cells the reference keeps the FP64 minimum (no float
+    rounding): the entry point must agree with tsu_reset there too."""
+    torch = pytest.importorskip("torch")
+    w = W.hump(40, 24, 10.0, sigma=60.0)
+    out = torch.full((2,), -1.0, dtype=torch.float64, device="cuda:0")
+    s = T.solver_for(w)
+    try:
+        _, dt0, _ = s.time()
+        assert _noalloc_dt(s, w.p, out.data_ptr()) == 0
+        assert _noalloc_dt(s, w.p, out.data_ptr() + 8) == 0
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+    finally:
+        s.close()
+    assert got[0] == dt0 and got[1] == dt0, (got, dt0)
+    assert float(np.float32(dt0)) != dt0  # the unrounded FP64 minimum
+
+
 def test_noalloc_rejects_grids_beyond_its_scratch():
     torch = pytest.importorskip("torch")
     w = W.hump(64, 48, 10.0)
@@ -62,6 +81,7 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
         rc = T.lib().tsu_cfl_dt_noalloc(C.c_void_p(ptr), C.c_void_p(ptr), C.c_void_p(ptr), 4096, C.byref(big),
                                         C.c_void_p(out.data_ptr()), None)
         assert rc == T.abi.TSU_ERR_INVALID
+        assert b"partial minima" in T.lib().tsu_last_error()
     finally:
         s.close()
     assert np.isfinite(float(out.cpu()[0]))

@@ -37,7 +37,7 @@ EXPORTS = [
     "tsu_corr_create", "tsu_corr_destroy", "tsu_corr_set_site", "tsu_corr_add_samples", "tsu_corr_num_samples",
     "tsu_corr_get_weights", "tsu_corr_set_weights", "tsu_corr_train", "tsu_corr_predict", "tsu_corr_bench_conv",
     "tsu_corr_last_train_ms", "tsu_corr_conv3x3", "tsu_corr_conv3x3_wgrad", "tsu_corr_status",
-    "tsu_corr_last_error",
+    "tsu_corr_last_error", "tsu_set_wait_limit_ns",
 ]
 
 _ENS_SIG = {
@@ -129,6 +129,7 @@ def lib():
             "tsu_struct_sizes": ([C.POINTER(C.c_size_t)], C.c_int),
             "tsu_parse_data_dat": ([C.c_char_p, C.POINTER(SimParams), C.c_char_p, C.c_char_p, C.c_char_p,
                                     C.c_char_p, C.POINTER(C.c_double), C.c_char_p, C.c_size_t], C.c_int),
+            "tsu_set_wait_limit_ns": ([C.c_ulonglong], C.c_int),
             "checkCUDAsupport": ([C.c_int], C.c_int),
             "initializeGPU": ([], None),
         }

@@ -49,12 +49,28 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-// waits for the phase of parity `parity` to complete; false after kWaitNs
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+// waits for the phase of parity `parity` to complete; false after `limit_ns`
+__device__ __forceinline__ bool mbar_wait_for(uint64_t *bar, unsigned parity, unsigned long long limit_ns) {
     const unsigned long long t0 = gtimer();
     while (!mbar_try(bar, parity))
-        if (gtimer() - t0 > kWaitNs) return false;
+        if (gtimer() - t0 > limit_ns) return false;
     return true;
+}
+// the wait that drains a CTA's own copies / MMAs on the error path: always
+// the full kWaitNs
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+    return mbar_wait_for(bar, parity, kWaitNs);
+}
+
+// Limit of a CTA's ordinary waits, whose expiry is reported as an error.  It
+// is kWaitNs unless a test lowers it (tsu_set_wait_limit_ns) to make those
+// waits run out while the copies are still in flight; the drain waits above
+// keep the full limit, so a CTA never leaves with its own copies or MMAs
+// still running.  One copy per compilation unit (set through that unit's
+// set_wait_limit_* host function on the current device).
+static __device__ unsigned long long g_wait_limit_ns = kWaitNs;
+__device__ __forceinline__ bool mbar_wait_first(uint64_t *bar, unsigned parity) {
+    return mbar_wait_for(bar, parity, *static_cast<volatile unsigned long long *>(&g_wait_limit_ns));
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");

@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __gr
         }
         if (prev >= 0) {  // epilogue of the previous tile overlaps this tile's loads
             const int j = i - 1;
-            const bool ok = mbar_wait(&mbar[j & 1], (j >> 1) & 1);
+            const bool ok = mbar_wait_first(&mbar[j & 1], (j >> 1) & 1);
             if (__syncthreads_or(!ok)) {
                 failed = true;
                 break;
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __gr
         fence_before();
         __syncthreads();
         fence_after();
-        if (tid == 0 && mbar_wait(&full[i % kFwdBufs], (i / kFwdBufs) & 1)) {
+        if (tid == 0 && mbar_wait_first(&full[i % kFwdBufs], (i / kFwdBufs) & 1)) {
             consumed = i;
             const uint32_t p_u32 = smem_u32(sP0 + (i % kFwdBufs) * kPatch);
             const uint32_t d = tmem + (uint32_t)((i & 1) * 32);
@@ -457,13 +457,13 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
         bool ok = true;
         const int tn = t + gridDim.x;
         if (tid == 0 && tn < G.total) {
-            if (i >= 1) ok = mbar_wait(&done[b ^ 1], ((i - 1) >> 1) & 1);
+            if (i >= 1) ok = mbar_wait_first(&done[b ^ 1], ((i - 1) >> 1) & 1);
             if (ok) {
                 issue(tn, b ^ 1);
                 last_load = i + 1;
             }
         }
-        const bool loaded = mbar_wait(&full[b], (i >> 1) & 1);
+        const bool loaded = mbar_wait_first(&full[b], (i >> 1) & 1);
         if (__syncthreads_or(!loaded || !ok)) {
             failed = true;
             break;
@@ -516,9 +516,12 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
         }
     } else if (n > 0) {
         const int L = n - 1;
-        const bool ok = mbar_wait(&done[L & 1], (L >> 1) & 1);
+        const bool ok = mbar_wait_first(&done[L & 1], (L >> 1) & 1);
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicExch(&g_corr_err, 1);
+            if (tid == 0) {
+                atomicExch(&g_corr_err, 1);
+                mbar_wait(&done[L & 1], (L >> 1) & 1);  // the MMAs before TMEM is freed
+            }
         } else {
             fence_after();
             if (warp < 3) {  // rows 0..95: dy = warp, cin = lane; rows 96..127 are ignored
@@ -760,6 +763,11 @@ cudaError_t wgrad_launch(const bf16 *X, const bf16 *dZ, int nimg, int H, int W, 
 }
 
 }  // namespace corr
+
+cudaError_t set_wait_limit_corrector(unsigned long long ns) {
+    return cudaMemcpyToSymbol(g_wait_limit_ns, &ns, sizeof(ns));
+}
+
 }  // namespace tsu
 
 using namespace tsu::corr;

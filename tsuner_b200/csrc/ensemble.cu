@@ -339,7 +339,15 @@ extern "C" int tsu_ens_sync(TsuEnsemble *E) {
     if (!E) return TSU_ERR_INVALID;
     ECK(cudaSetDevice(E->device));
     ECK(cudaStreamSynchronize(E->st));
-    return TSU_OK;
+    // every member's status words (an expired wait, a non-finite state)
+    int rc = TSU_OK;
+    for (TsuSolver *s : E->m) {
+        double sc[SC_N];
+        ECK(cudaMemcpy(sc, s->scal, sizeof(sc), cudaMemcpyDeviceToHost));
+        const int r = tsu_device_flags(s, sc);
+        if (r && !rc) rc = r;
+    }
+    return rc;
 }
 
 extern "C" int tsu_ens_last_step_ms(TsuEnsemble *E, double *ms) {
@@ -510,5 +518,5 @@ extern "C" int tsu_ens_run_until(TsuEnsemble *E, double t_end, long max_steps, l
     }
     if (rc) return rc;
     if (steps_done) *steps_done = done_steps;
-    return TSU_OK;
+    return tsu_ens_sync(E);  // the members' status words
 }

@@ -2,9 +2,10 @@
 // device allocation by the library.
 //
 // Some callers cannot let a library call cudaMalloc: code that runs inside a
-// host framework which owns all device memory through its own pool, code
-// that is captured into CUDA graphs where allocation calls are not allowed,
-// or embedded/long-running services that forbid allocation after start-up.
+// host framework which owns all device memory through its own pool (an
+// allocation behind its back can fail or fragment that pool), or embedded and
+// long-running services that forbid allocation after start-up so that memory
+// use stays fixed and no call can fail for lack of memory mid-run.
 // For them tsu_cfl_dt_noalloc() computes the reference's CFL step
 // (GetDeltaT + MinReduction, GPU/Volume_kernel.cu:19-43 and
 // GPU/Reduction_kernel_min.cu:155-196) of a state they already hold on the
@@ -18,6 +19,7 @@
 #include <mutex>
 
 #include "physics64.cuh"
+#include "solver.h"
 #include "stage64.h"
 #include "tsuner_b200.h"
 
@@ -90,10 +92,13 @@ extern "C" int tsu_cfl_dt_noalloc(const double *d_h, const double *d_qx, const d
         return TSU_ERR_INVALID;
     const long long ctas = (long long)((p->npx + kNoallocBx - 1) / kNoallocBx) * ((p->npy + kNoallocBy - 1) / kNoallocBy);
     if (ctas > kNoallocMaxCtas) {
-        std::fprintf(stderr,
-                     "tsu_cfl_dt_noalloc: a %d x %d grid needs %lld partial minima; the fixed scratch holds %d "
-                     "(at most %d cells); use tsu_create/tsu_reset for larger grids\n",
-                     p->npx, p->npy, ctas, kNoallocMaxCtas, kNoallocMaxCtas * kNoallocBx * kNoallocBy);
+        char msg[256];
+        std::snprintf(msg, sizeof(msg),
+                      "tsu_cfl_dt_noalloc: a %d x %d grid needs %lld partial minima; the fixed scratch holds %d "
+                      "(at most %d cells); use tsu_create/tsu_reset for larger grids",
+                      p->npx, p->npy, ctas, kNoallocMaxCtas, kNoallocMaxCtas * kNoallocBx * kNoallocBy);
+        tsu_set_error_detail(msg);
+        std::fprintf(stderr, "%s\n", msg);
         return TSU_ERR_INVALID;
     }
     int dev = 0;
@@ -107,7 +112,11 @@ extern "C" int tsu_cfl_dt_noalloc(const double *d_h, const double *d_qx, const d
             void *ptr = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
             if (e != cudaSuccess || !ptr) {
-                std::fprintf(stderr, "tsu_cfl_dt_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+                char msg[256];
+                std::snprintf(msg, sizeof(msg), "tsu_cfl_dt_noalloc: cudaGetSymbolAddress failed: %s",
+                              cudaGetErrorString(e));
+                tsu_set_error_detail(msg);
+                std::fprintf(stderr, "%s\n", msg);
                 return TSU_ERR_CUDA;
             }
             g_scratch_ptr[dev] = static_cast<double *>(ptr);

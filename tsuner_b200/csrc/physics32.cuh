@@ -41,6 +41,9 @@ struct Phys32 {
     float grass_ag;
 };
 
+// x is neither NaN nor an infinity (exponent field not all ones)
+__device__ __forceinline__ bool finite32(float x) { return (__float_as_uint(x) & 0x7f800000u) != 0x7f800000u; }
+
 // Reciprocal: the hardware approximation (at most 2 ulp for |x| in
 // [2^-126, 2^126]) refined by one Newton-Raphson step for 1/x,
 // r1 = r0 + r0 (1 - x r0), as two fused multiply-adds.  Every argument here

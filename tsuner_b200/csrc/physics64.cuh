@@ -48,6 +48,10 @@ __device__ __forceinline__ double ddiv_inf(double a, double b) {
     return ddiv(a, b);
 }
 
+// x is neither NaN nor an infinity (exponent field not all ones), with
+// integer instructions only (the FP64 pipe is the stage kernels' bottleneck)
+__device__ __forceinline__ bool finite64(double x) { return (__double2hiint(x) & 0x7ff00000) != 0x7ff00000; }
+
 // SGN (Sim_parameters.hxx:29)
 __device__ __forceinline__ int sgn(double x) { return (fabs(x) < kEpsilon) ? 0 : ((x) > 0) ? 1 : -1; }
 

@@ -50,6 +50,33 @@ __global__ void set_scal_kernel(double *scal, int i, double v) { scal[i] = v; }
 const char *tsu_last_error_detail() { return g_err; }
 void tsu_set_error_detail(const char *text) { snprintf(g_err, sizeof(g_err), "%s", text); }
 
+// Status words the kernels leave in the scalar block (the stream must be
+// synchronised): TSU_ERR_CUDA if a bounded wait expired, TSU_ERR_NONFINITE if
+// a cell became NaN / infinite.  Either one makes the solver need a
+// tsu_reset (after a new tsu_set_state for a non-finite state) before it steps
+// again: an expired wait leaves the step it happened in unfinished.
+int tsu_device_flags(TsuSolver *s, const double *sc) {
+    if (sc[SC_ERR] != 0.0) {
+        s->ready = false;
+        snprintf(g_err, sizeof(g_err), "a bounded device wait for a tile load expired (step %.0f); tsu_reset "
+                 "before stepping again", sc[SC_STEPS]);
+        return TSU_ERR_CUDA;
+    }
+    if (sc[SC_NAN] != 0.0) {
+        s->ready = false;
+        snprintf(g_err, sizeof(g_err), "the state holds a NaN or an infinite value (detected at step %.0f)",
+                 sc[SC_STEPS]);
+        return TSU_ERR_NONFINITE;
+    }
+    return TSU_OK;
+}
+
+static int device_flags(TsuSolver *s) {
+    double sc[SC_N];
+    CK(cudaMemcpy(sc, s->scal, sizeof(sc), cudaMemcpyDeviceToHost));
+    return tsu_device_flags(s, sc);
+}
+
 static int validate(const SimParams *p, const TsuSwitches *sw) {
     if (!p || !sw) return TSU_ERR_INVALID;
     if (p->npx < 1 || p->npy < 1 || (long long)p->npx * p->npy > (1LL << 31) - 1) return TSU_ERR_INVALID;
@@ -429,8 +456,12 @@ extern "C" int tsu_reset(TsuSolver *s) {
         return TSU_ERR_INVALID;
     }
     CK(cudaSetDevice(s->device));
-    double init[SC_N] = {0.0, -1.0, HUGE_VAL, 0.0, 0.0, 0.0, 0.0, 0.0};
+    s->ready = false;
+    double init[SC_N] = {0.0, -1.0, HUGE_VAL, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     CK(cudaMemcpyAsync(s->scal, init, sizeof(init), cudaMemcpyHostToDevice, s->st));
+    // the end-of-step ticket: a step whose tiles stopped early (an expired
+    // wait) leaves it short of the tile count
+    CK(cudaMemsetAsync(s->ticket, 0, sizeof(unsigned), s->st));
     if (s->fp32) {
         CK(fill32_launch((float *)s->hmax, s->plane, -1e30f, s->st));
         CK(fill32_launch((float *)s->bmin, s->plane, -1e30f, s->st));
@@ -445,6 +476,8 @@ extern "C" int tsu_reset(TsuSolver *s) {
                              s->st));
     }
     CK(cudaStreamSynchronize(s->st));
+    int rc = device_flags(s);  // e.g. a NaN in the uploaded state
+    if (rc) return rc;
     s->ready = true;
     return TSU_OK;
 }
@@ -503,22 +536,19 @@ extern "C" int tsu_step(TsuSolver *s, long nsteps) {
     return TSU_OK;
 }
 
-// TSU_ERR_CUDA if a kernel recorded an expired bounded wait (SC_ERR)
-static int device_wait_error(TsuSolver *s) {
-    double flag = 0.0;
-    CK(cudaMemcpy(&flag, s->scal + SC_ERR, sizeof(double), cudaMemcpyDeviceToHost));
-    if (flag != 0.0) {
-        snprintf(g_err, sizeof(g_err), "a bounded wait for a tile load expired on the device");
-        return TSU_ERR_CUDA;
-    }
-    return TSU_OK;
-}
-
 extern "C" int tsu_sync(TsuSolver *s) {
     if (!s) return TSU_ERR_INVALID;
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->st));
-    return device_wait_error(s);
+    return device_flags(s);
+}
+
+extern "C" int tsu_set_wait_limit_ns(unsigned long long ns) {
+    if (ns == 0) ns = kDefaultWaitNs;
+    CK(set_wait_limit_stage64(ns));
+    CK(set_wait_limit_stage32(ns));
+    CK(set_wait_limit_corrector(ns));
+    return TSU_OK;
 }
 
 extern "C" int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *steps_done) {
@@ -539,6 +569,7 @@ extern "C" int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *s
     set_scal_kernel<<<1, 1, 0, s->st>>>(s->scal, SC_TEND, t_end);
     CK(cudaGetLastError());
     long left = max_steps;
+    int rf = TSU_OK;
     while (left > 0) {
         long chunk = left < 64 ? left : 64;
         int r = tsu_step(s, chunk);
@@ -546,13 +577,14 @@ extern "C" int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *s
         left -= chunk;
         CK(cudaMemcpyAsync(sc, s->scal, sizeof(sc), cudaMemcpyDeviceToHost, s->st));
         CK(cudaStreamSynchronize(s->st));
+        if ((rf = tsu_device_flags(s, sc)) != TSU_OK) break;  // an expired wait or a non-finite state
         if (!(sc[SC_T] < t_end)) break;
     }
     set_scal_kernel<<<1, 1, 0, s->st>>>(s->scal, SC_TEND, HUGE_VAL);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s->st));
     if (steps_done) *steps_done = (long)(sc[SC_STEPS] - steps0);
-    return TSU_OK;
+    return rf;
 }
 
 void *TsuSolver::current() const {
@@ -623,7 +655,7 @@ extern "C" int tsu_get_time(TsuSolver *s, double *t, double *dt, long *steps) {
     if (t) *t = sc[SC_T];
     if (dt) *dt = sc[SC_DT];
     if (steps) *steps = (long)sc[SC_STEPS];
-    return device_wait_error(s);
+    return tsu_device_flags(s, sc);
 }
 
 extern "C" int tsu_get_sums(TsuSolver *s, double *water, double *sediment) {

@@ -48,6 +48,10 @@ struct TsuSolver {
     size_t elem() const { return fp32 ? sizeof(float) : sizeof(double); }
 };
 
+// status of the scalar block sc (a host copy of s->scal): TSU_OK, TSU_ERR_CUDA
+// (an expired device wait) or TSU_ERR_NONFINITE (a NaN / Inf state cell);
+// on an error the solver needs a tsu_reset before it steps again
+int tsu_device_flags(TsuSolver *s, const double *sc);
 const char *tsu_last_error_detail();
 // sets the detail text that tsu_last_error() returns on this thread
 void tsu_set_error_detail(const char *text);

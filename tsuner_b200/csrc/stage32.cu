@@ -231,7 +231,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     }
     __syncthreads();
     if (use_tma) {  // every thread sees the box land (bounded wait)
-        const bool ok = mbar_wait(&sBar, 0);
+        const bool ok = mbar_wait_first(&sBar, 0);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) {
                 A.scal[SC_ERR] = 1.0;
@@ -497,6 +497,7 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
     // ---- phase 5: update (state: z, H, qx, qy, hc)
     float dtcell = CUDART_INF_F;
     double mass = 0.0, sed = 0.0;
+    bool bad = false;  // last stage: the new state of the owned cell is not finite
     if (own) {
         float v0[5];
 #pragma unroll
@@ -592,10 +593,13 @@ __device__ __forceinline__ void stage32_tile(const Stage32Args &A, const Phys32 
             if (!isnan(d)) dtcell = d;
             mass = fmax(hd, 0.0);
             sed = (double)H + (double)hc;
+            bad = !(finite32(z) && finite32(H) && finite32(qx) && finite32(qy) && finite32(hc));
         }
     }
 
     if (LAST) {
+        // a NaN / Inf anywhere in the new state is reported to the host
+        if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0) A.scal[SC_NAN] = 1.0;
         // dt: the minimum of non-negative floats (or +inf) is the minimum of
         // their bit patterns, one warp reduction instruction
         const unsigned mb = __reduce_min_sync(0xffffffffu, __float_as_uint(dtcell));
@@ -750,7 +754,7 @@ __global__ void to32_kernel(const double *__restrict__ V64, long long pitch, lon
     const double h = V64[g], H = V64[3 * plane + g];
     const float Hf = (float)H;
     V32[plane + g] = Hf;
-    if (h > 0.0) {
+    if (!(h <= 0.0)) {  // wet, or a NaN depth (kept, so that tsu_reset reports it)
         V32[g] = (float)(h - (double)Hf - eta0);
         V32[2 * plane + g] = (float)V64[plane + g];
         V32[3 * plane + g] = (float)V64[2 * plane + g];
@@ -794,12 +798,16 @@ __global__ void __launch_bounds__(256) dt32_kernel(const float *__restrict__ V, 
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const int gi = blockIdx.x * blockDim.x + threadIdx.x, gj = blockIdx.y * blockDim.y + threadIdx.y;
     double m = CUDART_INF;
+    bool bad = false;
     if (gi < P.npx && gj < P.npy) {
         long long g = (long long)gj * pitch + gi;
         float h = (float)depth64(V[g], V[plane + g], P.eta0);
         float d = cfl_dt32(P, h, V[2 * plane + g], V[3 * plane + g]);
         if (!isnan(d)) m = d;
+        bad = !(finite32(V[g]) && finite32(V[plane + g]) && finite32(V[2 * plane + g]) &&
+                finite32(V[3 * plane + g]) && finite32(V[4 * plane + g]));
     }
+    if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0) scal[SC_NAN] = 1.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((tid & 31) == 0) sRed[tid >> 5] = m;
@@ -831,6 +839,10 @@ __global__ void __launch_bounds__(256) dt32_kernel(const float *__restrict__ V, 
 }
 
 // ------------------------------------------------------------------ host side
+cudaError_t set_wait_limit_stage32(unsigned long long ns) {
+    return cudaMemcpyToSymbol(g_wait_limit_ns, &ns, sizeof(ns));
+}
+
 namespace {
 
 struct Variant32 {

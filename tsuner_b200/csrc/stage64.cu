@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
     }
     __syncthreads();
     if (use_tma) {  // every thread sees the box land (bounded wait)
-        const bool ok = mbar_wait(&sBar, 0);
+        const bool ok = mbar_wait_first(&sBar, 0);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) {
                 A.scal[SC_ERR] = 1.0;
@@ -429,6 +429,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
 
     // ---- phase 5: cell update
     double dtcell = CUDART_INF;
+    bool bad = false;  // last stage: the new state of the owned cell is not finite
     if (own) {
         double vk[5];
 #pragma unroll
@@ -493,10 +494,14 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             if (h > eps_h) A.eta_max[gown] = fmax(A.eta_max[gown], h - z);
             double d = cfl_dt(P, h, qx, qy);
             if (!isnan(d)) dtcell = d;
+            bad = !(finite64(h) && finite64(qx) && finite64(qy) && finite64(z) && finite64(hc));
         }
     }
 
     if (LAST) {
+        // a NaN / Inf anywhere in the new state is reported to the host (the
+        // values themselves are stored unchanged, as the reference would)
+        if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0) A.scal[SC_NAN] = 1.0;
         // CTA minimum with warp shuffles; the last CTA to finish reduces the
         // partials, advances t and publishes the next dt
         // (GPU/main_TSUNER.cu:185,190-192).
@@ -551,11 +556,15 @@ __global__ void __launch_bounds__(256) dt_partials_kernel(const double *__restri
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const int gi = blockIdx.x * blockDim.x + threadIdx.x, gj = blockIdx.y * blockDim.y + threadIdx.y;
     double m = CUDART_INF;
+    bool bad = false;
     if (gi < P.npx && gj < P.npy) {
         long long g = (long long)gj * pitch + gi;
         double d = cfl_dt(P, V[g], V[plane + g], V[2 * plane + g]);
         if (!isnan(d)) m = d;
+        bad = !(finite64(V[g]) && finite64(V[plane + g]) && finite64(V[2 * plane + g]) &&
+                finite64(V[3 * plane + g]) && finite64(V[4 * plane + g]));
     }
+    if (__any_sync(0xffffffffu, bad) && (tid & 31) == 0) scal[SC_NAN] = 1.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((tid & 31) == 0) sRed[tid >> 5] = m;
@@ -614,6 +623,12 @@ __global__ void consts_kernel(SimParams p, TsuConsts *k) {
 }
 
 // ------------------------------------------------------------------ host side
+static_assert(kDefaultWaitNs == kWaitNs, "one default wait limit");
+
+cudaError_t set_wait_limit_stage64(unsigned long long ns) {
+    return cudaMemcpyToSymbol(g_wait_limit_ns, &ns, sizeof(ns));
+}
+
 EncodeTiledFn tensor_map_encoder() {
     static EncodeTiledFn f = [] {
         void *p = nullptr;

@@ -22,7 +22,20 @@ namespace tsu {
 //   [5] FP32 form: sum of water depth after the last step (FP64)
 //   [6] FP32 form: sum of H + hc after the last step (FP64)
 //   [7] non-zero when a bounded device wait expired (reported by the host)
-enum { SC_T = 0, SC_DT = 1, SC_TEND = 2, SC_STEPS = 3, SC_PAR = 4, SC_MASS = 5, SC_SED = 6, SC_ERR = 7, SC_N = 8 };
+//   [8] non-zero when a cell of the state became NaN or infinite (set by the
+//       last stage of a step and by the initial-dt kernel; reported by the host)
+enum {
+    SC_T = 0,
+    SC_DT = 1,
+    SC_TEND = 2,
+    SC_STEPS = 3,
+    SC_PAR = 4,
+    SC_MASS = 5,
+    SC_SED = 6,
+    SC_ERR = 7,
+    SC_NAN = 8,
+    SC_N = 9
+};
 
 struct Stage64Args {
     // TMA descriptors of the two state buffers as 3-D tensors [5][npy][npx]
@@ -63,6 +76,13 @@ cudaError_t initial_dt_launch(const double *V, long long pitch, long long plane,
 cudaError_t fill_launch(double *p, long long n, double v, cudaStream_t st);
 cudaError_t consts_launch(const SimParams &p, TsuConsts *k, cudaStream_t st);
 size_t partials_needed(int npx, int npy);
+// Limit of the ordinary bounded device waits of each kernel unit (the stage
+// kernels of stage64.cu / stage32.cu, the convolutions of corrector.cu), on
+// the current device; the error-path drain waits always keep the full limit.
+cudaError_t set_wait_limit_stage64(unsigned long long ns);
+cudaError_t set_wait_limit_stage32(unsigned long long ns);
+cudaError_t set_wait_limit_corrector(unsigned long long ns);
+constexpr unsigned long long kDefaultWaitNs = 500000000ull;  // async.cuh kWaitNs
 // encodes the TMA descriptors of the two FP64 state buffers for the current
 // tile shape; false if the driver cannot (the kernels then load with
 // ordinary instructions)
