@@ -75,7 +75,10 @@ enum {
  * reference ships with. */
 typedef struct TsuSwitches {
     int order;        /* 1 | 2                                   (`order`)   */
-    int rk;           /* 1 = Runge-Kutta (only 1 is implemented) (`RK`)      */
+    int rk;           /* 1 = Runge-Kutta; 0 = MUSCL-Hancock, one stage per
+                         step with the half-step predictor of
+                         GPU/Reconstructor.cu:280-342 (FP64 form only; the
+                         reference marks it "not fully tested")  (`RK`)      */
     int wbc;          /* 0 free | 1 wall | 2 periodic            (`WBC`)     */
     int bedload;      /* 0 | 1                                   (`BEDLOAD`) */
     int suspension;   /* 0 | 1                                   (`SUSPENSION`) */
@@ -90,6 +93,14 @@ typedef struct TsuSwitches {
     double eta0;      /* FP32 form: FP64 still-water level; the free surface is
                          stored as the FP32 deviation eta - eta0 (use the
                          sea level incl. sea-level rise)                      */
+    int manning;      /* 1 = the reference's Manning friction branch,
+                         GPU/Reconstructor.cu:47-50, as written there: the
+                         momentum is MULTIPLIED by c = dt FR^2 |u| / h^(4/3)
+                         (the reference marks it "NOT FINISHED, DO NOT USE";
+                         a dry cell gives 0/0).  FR is then the data.dat
+                         value (no /8, Problem_loader.cxx:337-339).  FP64
+                         form only.  0 = Chezy                   (`Manning`) */
+    int reserved;     /* 0 */
 } TsuSwitches;
 
 /* Per-run constants of the sediment laws, hoisted out of the per-cell code.

@@ -41,7 +41,8 @@ def lib():
         L.orc_initial_dt.restype = C.c_double
         L.orc_run.argtypes = [C.POINTER(SimParams), C.POINTER(TsuSwitches), C.c_void_p, _dp, _ip,
                               C.c_void_p, C.c_void_p, C.c_ulong, C.c_void_p, C.c_void_p, C.c_void_p,
-                              C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_long, C.c_double, C.c_int]
+                              C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_long, C.c_double, C.c_int,
+                              C.c_void_p]
         L.orc_run.restype = C.c_long
         L.orc_init_extrema.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_max_threads.restype = C.c_int
@@ -88,13 +89,15 @@ class OracleRun:
         self.t = C.c_double(0.0)
         self.dt = C.c_double(-1.0)
         self.steps = 0
+        # MUSCL-Hancock's unfiltered working state, carried across run() calls
+        self.Vk = self.V.copy()
 
     def run(self, nsteps=-1, t_end=0.0):
         k = None if self.k is None else C.byref(self.k)
         n = lib().orc_run(C.byref(self.p), C.byref(self.sw), k, self.V.reshape(-1), self.mask,
                           _ptr(self.CC), _ptr(self.tCC), self.timeCC, _ptr(self.hmax),
                           _ptr(self.bmin), _ptr(self.eta_max), C.byref(self.t), C.byref(self.dt),
-                          nsteps, t_end, self.nthreads)
+                          nsteps, t_end, self.nthreads, _ptr(self.Vk))
         if n < 0:
             raise RuntimeError("oracle run failed (%d)" % n)
         self.steps += n

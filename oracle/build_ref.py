@@ -33,7 +33,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_REF = "/root/reference"
+# the reference checkout: TSUNER_REF_DIR, else where this container mounts it
+DEFAULT_REF = os.environ.get("TSUNER_REF_DIR", "/root/reference")
 
 # name -> switch overrides (unset keys keep the reference defaults:
 # order 2, RK 1, WBC 1, BEDLOAD 1, SUSPENSION 1, Read_files 1)
@@ -44,6 +45,11 @@ VARIANTS = {
     "rf0_wbc2": {"Read_files": 0, "WBC": 2},
     "order1": {"order": 1},
     "nosed": {"BEDLOAD": 0, "SUSPENSION": 0},
+    # MUSCL-Hancock (GPU/Reconstructor.cu:280-342, one stage per step)
+    "rk0": {"RK": 0},
+    "rk0_order1": {"RK": 0, "order": 1},
+    # the unfinished Manning friction branch (GPU/Reconstructor.cu:47-50)
+    "manning_rf0": {"Manning": 1, "Read_files": 0},
 }
 
 KERNEL_SOURCES = [

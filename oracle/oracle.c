@@ -323,6 +323,7 @@ static void reconstruct(const Ctx *C, Bufs *B, double dT, double inv_dx, double 
                 rL[4 * nvol + pos] = (ci - 0.5 * du) * rL[pos];
                 rR[4 * nvol + pos] = (ci + 0.5 * du) * rR[pos];
                 Vk[1 * nvol + pos] -= dta * G_ * hi * deta;
+                const double Tpx = G_ * hi * deta; /* :199-201, used by RK == 0 */
 
                 /* y direction (:207-274) */
                 int jm = j - 1 * (j > 0), jp = j + 1 * (j < npy - 1);
@@ -365,6 +366,42 @@ static void reconstruct(const Ctx *C, Bufs *B, double dT, double inv_dx, double 
                 rD[4 * nvol + pos] = (ci - 0.5 * du) * rD[pos];
                 rU[4 * nvol + pos] = (ci + 0.5 * du) * rU[pos];
                 Vk[2 * nvol + pos] -= dta * G_ * hi * deta;
+                const double Tpy = G_ * hi * deta; /* :276-278 */
+
+                if (C->sw.rk == 0) {
+                    /* MUSCL-Hancock half-step predictor on the four unfiltered
+                     * faces, :280-342 (velocities from the faces before it) */
+                    double uRx, uRy, uLx, uLy, uUx, uUy, uDx, uDy;
+                    const long q1 = nvol + pos, q2 = 2 * nvol + pos, q3 = 3 * nvol + pos, q4 = 4 * nvol + pos;
+                    vel(rR[pos], rR[q1], rR[q2], &uRx, &uRy);
+                    vel(rL[pos], rL[q1], rL[q2], &uLx, &uLy);
+                    vel(rU[pos], rU[q1], rU[q2], &uUx, &uUy);
+                    vel(rD[pos], rD[q1], rD[q2], &uDx, &uDy);
+                    double qhx = (rR[q1] - rL[q1]) * inv_dx;
+                    double qhy = (rU[q2] - rD[q2]) * inv_dy;
+                    double up = 0.5 * dT * (qhx + qhy);
+                    rL[pos] -= up; rR[pos] -= up; rD[pos] -= up; rU[pos] -= up;
+                    qhx = (rR[q1] * uRx - rL[q1] * uLx) * inv_dx;
+                    qhy = (rU[q1] * uUy - rD[q1] * uDy) * inv_dy;
+                    up = 0.5 * dT * (qhx + qhy);
+                    rL[q1] -= up; rR[q1] -= up; rD[q1] -= up; rU[q1] -= up;
+                    qhx = (rR[q1] * uRy - rL[q1] * uLy) * inv_dx;
+                    qhy = (rU[q2] * uUy - rD[q2] * uDy) * inv_dy;
+                    up = 0.5 * dT * (qhx + qhy);
+                    rL[q2] -= up; rR[q2] -= up; rD[q2] -= up; rU[q2] -= up;
+                    qhx = (bedload(C, rR[pos], uRx, uRy) - bedload(C, rL[pos], uLx, uLy)) * inv_dx;
+                    qhy = (bedload(C, rU[pos], uUx, uUy) - bedload(C, rD[pos], uDx, uDy)) * inv_dy;
+                    up = 0.5 * dT * (qhx + qhy);
+                    rL[q3] -= up; rR[q3] -= up; rD[q3] -= up; rU[q3] -= up;
+                    qhx = (rR[q4] * uRx - rL[q4] * uLx) * inv_dx;
+                    qhy = (rU[q4] * uUy - rD[q4] * uDy) * inv_dy;
+                    up = 0.5 * dT * (qhx + qhy);
+                    rL[q4] -= up; rR[q4] -= up; rD[q4] -= up; rU[q4] -= up;
+                    up = 0.5 * dT * inv_dx * Tpx;
+                    rL[q1] -= up; rU[q1] -= up; rD[q1] -= up; rR[q1] -= up;
+                    up = 0.5 * dT * inv_dy * Tpy;
+                    rL[q2] -= up; rU[q2] -= up; rD[q2] -= up; rR[q2] -= up;
+                }
 
                 /* filters (:344-348) */
                 filt(&rL[pos], &rL[1 * nvol + pos], &rL[2 * nvol + pos], &rL[4 * nvol + pos]);
@@ -372,14 +409,21 @@ static void reconstruct(const Ctx *C, Bufs *B, double dT, double inv_dx, double 
                 filt(&rU[pos], &rU[1 * nvol + pos], &rU[2 * nvol + pos], &rU[4 * nvol + pos]);
                 filt(&rD[pos], &rD[1 * nvol + pos], &rD[2 * nvol + pos], &rD[4 * nvol + pos]);
             }
-            /* friction, :33-55 (Manning == 0) */
+            /* friction, :33-55: Chezy (Manning == 0) or the reference's
+             * unfinished Manning branch (:47-50), which multiplies by c */
             {
                 double h = V0[pos], ux, uy;
                 vel(h, V0[1 * nvol + pos], V0[2 * nvol + pos], &ux, &uy);
                 double modu = sqrt(ux * ux + uy * uy);
                 double c = dT * p->FR * modu / (h + EPSILON_);
-                Vk[1 * nvol + pos] /= (1.0 + c);
-                Vk[2 * nvol + pos] /= (1.0 + c);
+                if (C->sw.manning) {
+                    c = dT * p->FR * p->FR * modu / (pow(h, 4.0 / 3.0));
+                    Vk[1 * nvol + pos] *= c;
+                    Vk[2 * nvol + pos] *= c;
+                } else {
+                    Vk[1 * nvol + pos] /= (1.0 + c);
+                    Vk[2 * nvol + pos] /= (1.0 + c);
+                }
             }
             /* erosion_deposition, :57-88, calculate_erosion/deposition SedFlux.cuh:51-99 */
             {
@@ -526,7 +570,9 @@ static void volume_solver(const Ctx *C, Bufs *B, const int *fixH, double t, cons
     }
 }
 
-/* states_updater, GPU/Volume_kernel.cu:180-283 (RK == 1) */
+/* states_updater, GPU/Volume_kernel.cu:180-299: RK == 1 (:244-282) or
+ * RK == 0 (:283-299: V and V0 get the filtered state, Vk keeps the
+ * unfiltered one and carries it into the next step) */
 static void update(const Ctx *C, Bufs *B, int k, double invx, double invy)
 {
     const long nvol = B->nvol;
@@ -537,6 +583,13 @@ static void update(const Ctx *C, Bufs *B, int k, double invx, double invy)
         for (int f = 0; f < 5; f++) {
             long q = f * nvol + pos;
             Vk[q] -= invx * (FL[q] + FR[q]) + invy * (FD[q] + FU[q]);
+        }
+        if (C->sw.rk == 0) {
+            double h = Vk[pos], qx = Vk[nvol + pos], qy = Vk[2 * nvol + pos], hc = Vk[4 * nvol + pos];
+            filt(&h, &qx, &qy, &hc);
+            double out[5] = {h, qx, qy, Vk[3 * nvol + pos], hc};
+            for (int f = 0; f < 5; f++) V[f * nvol + pos] = V0[f * nvol + pos] = out[f];
+            continue;
         }
         double coef0 = 0.0 * (double)(k == 0) + 0.5 * (double)(k == 1);
         double coef1 = 1.0 - coef0;
@@ -609,13 +662,16 @@ double orc_initial_dt(const SimParams *p, const TsuSwitches *sw, const double *V
  * are the simulated time and the next step's dt, in/out (*dt < 0 on entry:
  * compute the initial dt first).  nsteps >= 0 runs exactly that many steps,
  * nsteps < 0 runs while t < t_end.  kin: device-evaluated constants, or NULL
- * for libm ones.  Returns the number of steps taken, or -1 on allocation
- * failure / -2 on an invalid boundary series.
+ * for libm ones.  Vk_io: the unfiltered working state that MUSCL-Hancock
+ * (RK == 0) carries from step to step, in/out (NULL: it starts equal to V,
+ * as at the start of the reference run, GPU/main_TSUNER.cu:113-115).
+ * Returns the number of steps taken, or -1 on allocation failure / -2 on an
+ * invalid boundary series.
  */
 long orc_run(const SimParams *p, const TsuSwitches *sw, const TsuConsts *kin, double *V,
              const int *fixH, const double *CC, const double *tCC, unsigned long timeCC,
              double *hmax, double *bmin, double *eta_max, double *t, double *dt, long nsteps,
-             double t_end, int nthreads)
+             double t_end, int nthreads, double *Vk_io)
 {
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -639,14 +695,16 @@ long orc_run(const SimParams *p, const TsuSwitches *sw, const TsuConsts *kin, do
     B.dtv = mem + 10 * n5;
     memset(B.FL, 0, sizeof(double) * n5 * 4);
     memcpy(B.V0, V, sizeof(double) * n5);
-    memcpy(B.Vk, V, sizeof(double) * n5);
+    memcpy(B.Vk, Vk_io ? Vk_io : V, sizeof(double) * n5);
     double inv_dx = 1.0 / p->dx, inv_dy = 1.0 / p->dy;
     double dT = *dt;
     if (dT < 0) dT = get_dt(&C, V, B.nvol);
     double ct = *t;
     long it = 0;
+    /* GPU/main_TSUNER.cu:169-174: `order` RK stages, or one MUSCL-Hancock stage */
+    const int nstages = (sw->rk == 0) ? 1 : sw->order;
     while (nsteps >= 0 ? it < nsteps : ct < t_end) {
-        for (int k = 0; k < sw->order; k++) {
+        for (int k = 0; k < nstages; k++) {
             reconstruct(&C, &B, dT, inv_dx, inv_dy);
             volume_solver(&C, &B, fixH, ct, CC, tCC, timeCC);
             update(&C, &B, k, dT * inv_dx, dT * inv_dy);
@@ -669,6 +727,7 @@ long orc_run(const SimParams *p, const TsuSwitches *sw, const TsuConsts *kin, do
     }
     *t = ct;
     *dt = dT;
+    if (Vk_io) memcpy(Vk_io, B.Vk, sizeof(double) * n5);
     free(mem);
     return it;
 }

@@ -40,11 +40,19 @@ CASES = {
     "nosed_40x24": ("nosed", lambda: W.nwave_shelf(40, 24, 40.0, slr=0.5, amp=2.0, period=200.0, t_series=150.0),
                     dict(order=2, wbc=1, read_files=1, bedload=0, suspension=0), 50),
     "above4096_72x64": ("default", lambda: W.hump(72, 64, 10.0, sigma=120.0), dict(order=2, wbc=1, read_files=0), 30),
+    "hancock_nwave_48x36": ("rk0", lambda: W.nwave_shelf(48, 36, 40.0, slr=0.5, amp=2.0, period=200.0,
+                                                         t_series=150.0), dict(order=2, wbc=1, read_files=1, rk=0), 60),
+    "hancock_o1_40x24": ("rk0_order1", lambda: W.nwave_shelf(40, 24, 40.0, slr=0.5, amp=2.0, period=200.0,
+                                                             t_series=150.0), dict(order=1, wbc=1, read_files=1, rk=0),
+                         50),
+    "manning_hump_40x30": ("manning_rf0", lambda: W.hump(40, 30, 10.0, sigma=70.0),
+                           dict(order=2, wbc=1, read_files=0, manning=1), 40),
 }
 
 PFIELDS = ["xmin", "xmax", "ymin", "ymax", "total_time", "save_time", "npx", "npy", "nvol", "CFL", "Q", "R",
            "porosity", "DS", "FR", "Opar", "OC", "Dsg", "HQB", "vmax", "epsilon_h", "dx", "dy"]
-SFIELDS = ["order", "rk", "wbc", "bedload", "suspension", "read_files", "bedload_law", "precision", "grass_ag"]
+SFIELDS = ["order", "rk", "wbc", "bedload", "suspension", "read_files", "bedload_law", "precision", "grass_ag",
+           "manning"]
 KFIELDS = ["vs", "Rp", "A_er", "sqrt_FR", "VP", "K_dep", "sqrt_OC", "DS5"]
 
 

@@ -103,6 +103,7 @@ def test_dt_float_rounding_above_4096_cells():
 @pytest.mark.parametrize("variant", [
     dict(order=1, wbc=1), dict(order=2, wbc=0), dict(order=2, wbc=2),
     dict(order=2, wbc=1, bedload=0, suspension=0), dict(order=2, wbc=1, bedload_law=1, grass_ag=1e-3),
+    dict(order=2, wbc=1, rk=0), dict(order=1, wbc=1, rk=0), dict(order=2, wbc=1, manning=1),
 ])
 def test_switch_variants_run(variant):
     w = W.hump(40, 32, 10.0, sigma=80.0)
@@ -110,6 +111,38 @@ def test_switch_variants_run(variant):
     r.run(30)
     assert np.isfinite(r.V).all()
     assert (r.V[0] >= 0).all()
+
+
+def test_muscl_hancock_state_carried_across_runs():
+    """MUSCL-Hancock keeps the reference's unfiltered working state Vk from
+    step to step (GPU/Volume_kernel.cu:283-299): runs split over several calls
+    equal one run, and the result differs from the RK2 scheme's."""
+    w = W.nwave_shelf(40, 30, 40.0, slr=0.5, amp=2.0, period=200.0, t_series=150.0)
+    sw = make_switches(order=2, wbc=1, read_files=1, rk=0)
+    one = oracle.OracleRun(w.p, sw, w.V, w.mask, w.CC, w.tCC)
+    one.run(25)
+    parts = oracle.OracleRun(w.p, sw, w.V, w.mask, w.CC, w.tCC)
+    for n in (3, 10, 12):
+        parts.run(n)
+    assert np.array_equal(one.V, parts.V) and one.t.value == parts.t.value
+    assert not np.array_equal(one.Vk, one.V)  # the filter rounds; Vk keeps the unfiltered values
+    rk2 = oracle.OracleRun(w.p, make_switches(order=2, wbc=1, read_files=1), w.V, w.mask, w.CC, w.tCC)
+    rk2.run(25)
+    assert not np.array_equal(one.V, rk2.V)
+
+
+def test_manning_branch_multiplies_momentum():
+    """GPU/Reconstructor.cu:47-50 as written: q *= dt FR^2 |u| / h^(4/3), so on
+    a wet grid every step scales the carried momentum by that (small) factor
+    before the fluxes act, and momentum does not build up as with Chezy."""
+    w = W.hump(30, 24, 10.0, sigma=60.0)
+    sw = make_switches(order=1, wbc=1, manning=1, bedload=0, suspension=0)
+    r = oracle.OracleRun(w.p, sw, w.V, w.mask)
+    r.run(5)
+    rc = oracle.OracleRun(w.p, make_switches(order=1, wbc=1, bedload=0, suspension=0), w.V, w.mask)
+    rc.run(5)
+    assert np.isfinite(r.V).all()
+    assert np.abs(r.V[1]).max() < 0.5 * np.abs(rc.V[1]).max()
 
 
 def test_boundary_series_nwave_enters():

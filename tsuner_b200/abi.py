@@ -33,6 +33,7 @@ class TsuSwitches(C.Structure):
         ("order", C.c_int), ("rk", C.c_int), ("wbc", C.c_int), ("bedload", C.c_int),
         ("suspension", C.c_int), ("read_files", C.c_int), ("bedload_law", C.c_int),
         ("precision", C.c_int), ("grass_ag", C.c_double), ("eta0", C.c_double),
+        ("manning", C.c_int), ("reserved", C.c_int),
     ]
 
 
@@ -70,9 +71,10 @@ def make_params(npx, npy, dx, dy, *, CFL=0.9, epsilon_h=1e-4, R=2.6, DS=2e-4, fr
 
 
 def make_switches(order=2, wbc=1, bedload=1, suspension=1, read_files=0, bedload_law=0,
-                  precision=0, grass_ag=1e-3, rk=1, eta0=0.0):
+                  precision=0, grass_ag=1e-3, rk=1, eta0=0.0, manning=0):
     s = TsuSwitches()
     s.eta0 = eta0
+    s.manning = manning
     s.order, s.rk, s.wbc, s.bedload, s.suspension = order, rk, wbc, bedload, suspension
     s.read_files, s.bedload_law, s.precision, s.grass_ag = read_files, bedload_law, precision, grass_ag
     return s

@@ -30,6 +30,7 @@ struct Phys64 {
     int npx, npy;
     int order, wbc, bedload, suspension, read_files, bedload_law;
     double grass_ag;
+    int rk, manning;
 };
 
 // IEEE quotient and square root with the zero cases answered directly:
@@ -229,6 +230,70 @@ __device__ __forceinline__ void edge_flux(const Phys64 &P, const State5 &a, cons
     Dp[2] = (dny * p[1] + dnx * p[2]);
     Dp[3] = p[3];
     Dp[4] = p[4];
+}
+
+// MUSCL-Hancock half-step predictor (RK == 0, GPU/Reconstructor.cu:280-342)
+// on a cell's four faces before the state filter: L/R along x, D/U along y.
+// hi is the cell's depth, detx/dety its hydrostatic slopes (the pressure
+// terms Tpx/Tpy of :199-201,276-278).  The face velocities are taken once,
+// before any face is updated, and each update reads the faces as the
+// previous ones left them -- the order of the reference.  Its bedload terms
+// use bedload() directly (no mask, no BEDLOAD switch), as the reference does.
+__device__ __forceinline__ void hancock_predictor(const Phys64 &P, double dt, double hi, double detx, double dety,
+                                                  State5 &L, State5 &R, State5 &D, State5 &U) {
+    const double Tpx = kG * hi * detx;
+    const double Tpy = kG * hi * dety;
+    double uRx, uRy, mR, uLx, uLy, mL, uUx, uUy, mU, uDx, uDy, mD;
+    velocity(R.h, R.qx, R.qy, uRx, uRy, mR);
+    velocity(L.h, L.qx, L.qy, uLx, uLy, mL);
+    velocity(U.h, U.qx, U.qy, uUx, uUy, mU);
+    velocity(D.h, D.qx, D.qy, uDx, uDy, mD);
+    const double hdt = 0.5 * dt;
+    double qhx = (R.qx - L.qx) * P.inv_dx;
+    double qhy = (U.qy - D.qy) * P.inv_dy;
+    double up = hdt * (qhx + qhy);
+    L.h -= up;
+    R.h -= up;
+    D.h -= up;
+    U.h -= up;
+    qhx = (R.qx * uRx - L.qx * uLx) * P.inv_dx;
+    qhy = (U.qx * uUy - D.qx * uDy) * P.inv_dy;
+    up = hdt * (qhx + qhy);
+    L.qx -= up;
+    R.qx -= up;
+    D.qx -= up;
+    U.qx -= up;
+    qhx = (R.qx * uRy - L.qx * uLy) * P.inv_dx;
+    qhy = (U.qy * uUy - D.qy * uDy) * P.inv_dy;
+    up = hdt * (qhx + qhy);
+    L.qy -= up;
+    R.qy -= up;
+    D.qy -= up;
+    U.qy -= up;
+    qhx = (bedload_flux(P, R.h, uRx, mR) - bedload_flux(P, L.h, uLx, mL)) * P.inv_dx;
+    qhy = (bedload_flux(P, U.h, uUx, mU) - bedload_flux(P, D.h, uDx, mD)) * P.inv_dy;
+    up = hdt * (qhx + qhy);
+    L.H -= up;
+    R.H -= up;
+    D.H -= up;
+    U.H -= up;
+    qhx = (R.hc * uRx - L.hc * uLx) * P.inv_dx;
+    qhy = (U.hc * uUy - D.hc * uDy) * P.inv_dy;
+    up = hdt * (qhx + qhy);
+    L.hc -= up;
+    R.hc -= up;
+    D.hc -= up;
+    U.hc -= up;
+    up = hdt * P.inv_dx * Tpx;
+    L.qx -= up;
+    U.qx -= up;
+    D.qx -= up;
+    R.qx -= up;
+    up = hdt * P.inv_dy * Tpy;
+    L.qy -= up;
+    U.qy -= up;
+    D.qy -= up;
+    R.qy -= up;
 }
 
 // interpolate_time (GPU/VolumeSolver.cu:172-203): boundary state from the

@@ -82,7 +82,10 @@ static int validate(const SimParams *p, const TsuSwitches *sw) {
     if (p->npx < 1 || p->npy < 1 || (long long)p->npx * p->npy > (1LL << 31) - 1) return TSU_ERR_INVALID;
     if (!(p->dx > 0) || !(p->dy > 0) || !(p->CFL > 0)) return TSU_ERR_INVALID;
     if (sw->order != 1 && sw->order != 2) return TSU_ERR_INVALID;
-    if (sw->rk != 1) return TSU_ERR_INVALID;
+    if (sw->rk != 0 && sw->rk != 1) return TSU_ERR_INVALID;
+    if (sw->manning != 0 && sw->manning != 1) return TSU_ERR_INVALID;
+    // MUSCL-Hancock and the Manning branch exist in the FP64 plain form only
+    if (sw->precision == 1 && (sw->rk == 0 || sw->manning)) return TSU_ERR_INVALID;
     if (sw->wbc < 0 || sw->wbc > 2) return TSU_ERR_INVALID;
     if (sw->bedload_law < 0 || sw->bedload_law > 1) return TSU_ERR_INVALID;
     if (sw->precision != 0 && sw->precision != 1) return TSU_ERR_INVALID;
@@ -122,6 +125,7 @@ static void free_all(TsuSolver *s) {
     s->invalidate_graph();
     cudaFree(s->A);
     cudaFree(s->B);
+    cudaFree(s->K);
     cudaFree(s->hmax);
     cudaFree(s->bmin);
     cudaFree(s->eta);
@@ -164,6 +168,8 @@ static void fill_phys(TsuSolver *s) {
     P.read_files = sw->read_files;
     P.bedload_law = sw->bedload_law;
     P.grass_ag = sw->grass_ag;
+    P.rk = sw->rk;
+    P.manning = sw->manning;
     Phys32 &Q = s->phys32;
     Q.eta0 = sw->eta0;
     Q.eta0f = (float)sw->eta0;
@@ -229,6 +235,7 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
     if (e == cudaSuccess) e = cudaMalloc((void **)&(ptr), (bytes));
     AL(s->A, 5 * pl);
     AL(s->B, 5 * pl);
+    if (sw->rk == 0) AL(s->K, 5 * pl);
     AL(s->hmax, pl);
     AL(s->bmin, pl);
     AL(s->eta, pl);
@@ -402,6 +409,7 @@ Stage64Args TsuSolver::args() const {
     Stage64Args a;
     a.bufA = (double *)A;
     a.bufB = (double *)B;
+    a.bufK = (double *)K;
     a.mask = mask;
     a.CC = CC;
     a.tCC = tCC;
@@ -457,6 +465,14 @@ extern "C" int tsu_reset(TsuSolver *s) {
     }
     CK(cudaSetDevice(s->device));
     s->ready = false;
+    const size_t state_bytes = 5 * (size_t)s->plane * s->elem();
+    if (s->single_stage()) {
+        // the state may sit in B after an odd number of single-stage steps:
+        // bring it to A, where a reset run starts
+        CK(cudaStreamSynchronize(s->st));
+        if (s->current() == s->B) CK(cudaMemcpyAsync(s->A, s->B, state_bytes, cudaMemcpyDeviceToDevice, s->st));
+    }
+    if (s->K) CK(cudaMemcpyAsync(s->K, s->A, state_bytes, cudaMemcpyDeviceToDevice, s->st));  // Vk = V
     double init[SC_N] = {0.0, -1.0, HUGE_VAL, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     CK(cudaMemcpyAsync(s->scal, init, sizeof(init), cudaMemcpyHostToDevice, s->st));
     // the end-of-step ticket: a step whose tiles stopped early (an expired
@@ -495,7 +511,7 @@ int TsuSolver::launch_steps(long n) {
     } else {
         Stage64Args a = args();
         for (long i = 0; i < n; i++)
-            for (int k = 0; k < sw.order; k++) CK(stage64_launch(sw.order, k, a, st));
+            for (int k = 0; k < stages(); k++) CK(stage64_launch(sw.order, k, a, st));
     }
     return TSU_OK;
 }
@@ -531,7 +547,7 @@ extern "C" int tsu_step(TsuSolver *s, long nsteps) {
     int r = s->launch_steps(n);
     if (r) return r;
     CK(cudaEventRecord(s->e1, s->st));
-    s->last_launches = nsteps * s->sw.order;
+    s->last_launches = nsteps * s->stages();
     s->timed = true;
     return TSU_OK;
 }
@@ -588,7 +604,7 @@ extern "C" int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *s
 }
 
 void *TsuSolver::current() const {
-    if (sw.order == 2) return A;
+    if (!single_stage()) return A;
     double sc[SC_N];
     if (cudaMemcpy(sc, scal, sizeof(sc), cudaMemcpyDeviceToHost) != cudaSuccess) return A;
     return sc[SC_PAR] != 0.0 ? B : A;

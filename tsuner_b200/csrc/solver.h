@@ -17,6 +17,7 @@ struct TsuSolver {
     long long pitch = 0, plane = 0;  // elements
     // FP64 plain form: planes h, qx, qy, H, hc.  FP32 form: z, H, qx, qy, hc.
     void *A = nullptr, *B = nullptr;
+    void *K = nullptr;  // MUSCL-Hancock (rk == 0) only: the unfiltered working state Vk
     void *hmax = nullptr, *bmin = nullptr, *eta = nullptr;
     double *stage64 = nullptr;  // FP32 form: FP64 staging planes for upload/download
     unsigned char *mask = nullptr;
@@ -46,6 +47,9 @@ struct TsuSolver {
     void invalidate_graph();
     void *current() const;
     size_t elem() const { return fp32 ? sizeof(float) : sizeof(double); }
+    // one kernel per step whose state alternates between A and B (order 1, MUSCL-Hancock)
+    bool single_stage() const { return sw.order == 1 || sw.rk == 0; }
+    int stages() const { return single_stage() ? 1 : sw.order; }
 };
 
 // status of the scalar block sc (a host copy of s->scal): TSU_OK, TSU_ERR_CUDA

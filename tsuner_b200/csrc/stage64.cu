@@ -66,8 +66,9 @@ __device__ __forceinline__ int wrap_clamp(int g, int n, bool periodic) {
 
 // MUSCL reconstruction of one cell along one direction, GPU/Reconstructor.cu
 // :124-194 (x) / :207-271 (y).  c/l/r index the centre and its two
-// neighbours in the smem tile (plane stride PS).  Returns the two filtered
-// faces (minus side, plus side) and the hydrostatic slope deta.
+// neighbours in the smem tile (plane stride PS).  Returns the two faces
+// (minus side, plus side) before the state filter and the hydrostatic slope
+// deta.
 template <int PS>
 __device__ __forceinline__ void reconstruct_dir(const double *sV, const double *sUC, int c, int l, int r,
                                                 State5 &fm, State5 &fp, double &deta) {
@@ -113,10 +114,9 @@ __device__ __forceinline__ void reconstruct_dir(const double *sV, const double *
     du = limiter(dl, dr);
     fm.hc = (ci - 0.5 * du) * fm.h;
     fp.hc = (ci + 0.5 * du) * fp.h;
-
-    positivity_filter(fm.h, fm.qx, fm.qy, fm.hc);
-    positivity_filter(fp.h, fp.qx, fp.qy, fp.hc);
 }
+
+__device__ __forceinline__ void filter5(State5 &s) { positivity_filter(s.h, s.qx, s.qy, s.hc); }
 
 __device__ __forceinline__ void put5(double *base, int stride, const State5 &s) {
     base[0] = s.h;
@@ -139,8 +139,14 @@ __device__ __forceinline__ void put5a(double *base, int stride, const double D[5
     for (int f = 0; f < 5; f++) base[f * stride] = D[f];
 }
 
-template <int TX, int TY, int NTHR, int MINB, int ORDER, bool FIRST, bool LAST>
+// RK0: MUSCL-Hancock (RK == 0 of the reference): one stage per step
+// (FIRST = LAST = true), the state ping-pongs between bufA and bufB like the
+// order-1 form, and bufK holds the unfiltered working state Vk that the
+// reference carries from step to step (GPU/Volume_kernel.cu:283-299).
+template <int TX, int TY, int NTHR, int MINB, int ORDER, bool FIRST, bool LAST, bool RK0 = false>
 __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_constant__ Stage64Args A) {
+    static_assert(!RK0 || (FIRST && LAST), "MUSCL-Hancock is a single stage");
+    constexpr bool PINGPONG = (ORDER == 1) || RK0;
     using T = Tile<TX, TY, NTHR>;
     constexpr int NT = T::NT, LX = T::LX, LY = T::LY, PS = T::PS, FXW = T::FXW, FYH = T::FYH;
     constexpr int MHX = T::MHX, MLX = T::MLX;
@@ -172,7 +178,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
     const double *V0;
     double *Vout;
     int par = 0;
-    if (ORDER == 2) {
+    if (!PINGPONG) {
         Vin = FIRST ? A.bufA : A.bufB;
         V0 = A.bufA;
         Vout = FIRST ? A.bufB : A.bufA;
@@ -260,7 +266,52 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
 
     // ---- phase 3: faces (one reconstruction call site)
     constexpr int NXI = FXW * TY, NYI = TX * FYH;
-    for (int item = tid; item < NXI + NYI; item += NT) {
+    if (RK0 && ORDER == 2) {
+        // MUSCL-Hancock: the predictor needs all four faces of a cell, so an
+        // item is a cell -- the tile, then its halo columns -1 / TX (x faces
+        // kept) and halo rows -1 / TY (y faces kept)
+        constexpr int NC = TX * TY + 2 * TY + 2 * TX;
+        for (int item = tid; item < NC; item += NT) {
+            int lx, ly;
+            if (item < TX * TY) {
+                ly = item / TX;
+                lx = item - ly * TX;
+            } else if (item < TX * TY + 2 * TY) {
+                const int k = item - TX * TY;
+                ly = k >> 1;
+                lx = (k & 1) ? TX : -1;
+            } else {
+                const int k = item - TX * TY - 2 * TY;
+                lx = k >> 1;
+                ly = (k & 1) ? TY : -1;
+            }
+            const int c = (ly + 2) * LX + (lx + 2);
+            State5 L, R, D, U;
+            double detx, dety;
+            reconstruct_dir<PS>(sV, sUC, c, c - 1, c + 1, L, R, detx);
+            reconstruct_dir<PS>(sV, sUC, c, c - LX, c + LX, D, U, dety);
+            hancock_predictor(P, dt, sV[c], detx, dety, L, R, D, U);
+            filter5(L);
+            filter5(R);
+            filter5(U);
+            filter5(D);
+            if (ly >= 0 && ly < TY) {
+                double *dst = sFx + ly * FXW + (lx + 1);
+                put5(dst, TY * FXW, L);
+                put5(dst + 5 * TY * FXW, TY * FXW, R);
+            }
+            if (lx >= 0 && lx < TX) {
+                double *dst = sFy + (ly + 1) * TX + lx;
+                put5(dst, FYH * TX, D);
+                put5(dst + 5 * FYH * TX, FYH * TX, U);
+            }
+            if (lx >= 0 && lx < TX && ly >= 0 && ly < TY) {
+                sDeta[ly * TX + lx] = detx;
+                sDeta[TY * TX + ly * TX + lx] = dety;
+            }
+        }
+    }
+    for (int item = tid; item < ((RK0 && ORDER == 2) ? 0 : NXI + NYI); item += NT) {
         int c, step, fstride, side, didx = -1;
         double *dst;
         if (item < NXI) {
@@ -287,6 +338,8 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
         if (ORDER == 2) {
             double deta;
             reconstruct_dir<PS>(sV, sUC, c, c - step, c + step, fm, fp, deta);
+            filter5(fm);  // GPU/Reconstructor.cu:344-348
+            filter5(fp);
             if (didx >= 0) sDeta[didx] = deta;
         } else {  // first order: faces are the cell values (GPU/Reconstructor.cu:99-107)
             fm = get5(sV + c, PS);
@@ -431,9 +484,9 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
     double dtcell = CUDART_INF;
     bool bad = false;  // last stage: the new state of the owned cell is not finite
     if (own) {
-        double vk[5];
+        double vk[5];  // the reference's Vk: this stage's input, or MUSCL-Hancock's carried working state
 #pragma unroll
-        for (int f = 0; f < 5; f++) vk[f] = vc[f];
+        for (int f = 0; f < 5; f++) vk[f] = RK0 ? A.bufK[f * plane + gown] : vc[f];
         if (ORDER == 2) {  // pressure source, GPU/Reconstructor.cu:197,274
             const double dtax = dt * P.inv_dx, dtay = dt * P.inv_dy;
             vk[1] -= dtax * kG * vc[0] * sDeta[ty * TX + tx];
@@ -445,9 +498,15 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             double ux, uy;
             velocity(v0[0], v0[1], v0[2], ux, uy);
             double modu = dsqrt(ux * ux + uy * uy);
-            double cf = ddiv(dt * P.FR * modu, v0[0] + kEpsilon);
-            vk[1] = ddiv(vk[1], 1.0 + cf);
-            vk[2] = ddiv(vk[2], 1.0 + cf);
+            if (P.manning) {  // GPU/Reconstructor.cu:47-50 as written (multiplies)
+                const double cm = dt * P.FR * P.FR * modu / pow(v0[0], 4.0 / 3.0);
+                vk[1] *= cm;
+                vk[2] *= cm;
+            } else {
+                double cf = ddiv(dt * P.FR * modu, v0[0] + kEpsilon);
+                vk[1] = ddiv(vk[1], 1.0 + cf);
+                vk[2] = ddiv(vk[2], 1.0 + cf);
+            }
             double c = ddiv(v0[4], v0[0] + P.eps_h);
             double Z = ddiv(P.k.A_er * (modu * P.k.sqrt_FR), P.k.vs);
             double Z5 = Z * Z * Z * Z * Z;
@@ -472,15 +531,27 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             double FD = sFlux[(2 * 5 + f) * FS + cell], FU = sFlux[(3 * 5 + f) * FS + cell];
             vk[f] -= invx * (FL + FR) + invy * (FD + FU);
         }
-        // RK combine + filter, GPU/Volume_kernel.cu:244-281
-        const int k = (ORDER == 2 && !FIRST) ? 1 : 0;
-        const double coef0 = 0.0 * (double)(k == 0) + 0.5 * (double)(k == 1);
-        const double coef1 = 1.0 - coef0;
-        double h = coef0 * v0[0] + coef1 * vk[0];
-        double qx = coef0 * v0[1] + coef1 * vk[1];
-        double qy = coef0 * v0[2] + coef1 * vk[2];
-        double z = coef0 * v0[3] + coef1 * vk[3];
-        double hc = coef0 * v0[4] + coef1 * vk[4];
+        // RK combine + filter, GPU/Volume_kernel.cu:244-281; MUSCL-Hancock
+        // filters Vk itself and keeps the unfiltered Vk (:283-299)
+        double h, qx, qy, z, hc;
+        if (RK0) {
+            h = vk[0];
+            qx = vk[1];
+            qy = vk[2];
+            z = vk[3];
+            hc = vk[4];
+#pragma unroll
+            for (int f = 0; f < 5; f++) A.bufK[f * plane + gown] = vk[f];
+        } else {
+            const int k = (ORDER == 2 && !FIRST) ? 1 : 0;
+            const double coef0 = 0.0 * (double)(k == 0) + 0.5 * (double)(k == 1);
+            const double coef1 = 1.0 - coef0;
+            h = coef0 * v0[0] + coef1 * vk[0];
+            qx = coef0 * v0[1] + coef1 * vk[1];
+            qy = coef0 * v0[2] + coef1 * vk[2];
+            z = coef0 * v0[3] + coef1 * vk[3];
+            hc = coef0 * v0[4] + coef1 * vk[4];
+        }
         positivity_filter(h, qx, qy, hc);
         Vout[gown] = h;
         Vout[plane + gown] = qx;
@@ -539,7 +610,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
                 A.scal[SC_T] = t + dt;
                 A.scal[SC_DT] = finalize_dt(mm, (long long)npx * npy);
                 A.scal[SC_STEPS] += 1.0;
-                if (ORDER == 1) A.scal[SC_PAR] = (double)(1 - par);
+                if (PINGPONG) A.scal[SC_PAR] = (double)(1 - par);
                 *A.ticket = 0u;
                 __threadfence();
             }
@@ -646,7 +717,8 @@ namespace {
 struct Variant {
     int tx, ty, nthr;
     size_t smem;
-    void (*k[3])(Stage64Args);  // order2 stage0, order2 stage1, order1
+    // order2 stage0, order2 stage1, order1, MUSCL-Hancock order2, MUSCL-Hancock order1
+    void (*k[5])(Stage64Args);
 };
 
 template <int TX, int TY, int MINB, int NTHR = TX * TY>
@@ -659,6 +731,8 @@ Variant make_variant() {
     v.k[0] = stage64_kernel<TX, TY, NTHR, MINB, 2, true, false>;
     v.k[1] = stage64_kernel<TX, TY, NTHR, MINB, 2, false, true>;
     v.k[2] = stage64_kernel<TX, TY, NTHR, MINB, 1, true, true>;
+    v.k[3] = stage64_kernel<TX, TY, NTHR, MINB, 2, true, true, true>;
+    v.k[4] = stage64_kernel<TX, TY, NTHR, MINB, 1, true, true, true>;
     return v;
 }
 
@@ -688,7 +762,7 @@ size_t stage64_smem_bytes() { return variant().smem; }
 
 cudaError_t stage64_prepare() {
     const Variant &v = variant();
-    for (int i = 0; i < 3; i++) {
+    for (int i = 0; i < 5; i++) {
         cudaError_t e = cudaFuncSetAttribute(v.k[i], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
         if (e != cudaSuccess) return e;
     }
@@ -733,6 +807,7 @@ cudaError_t stage64_launch(int order, int stage, const Stage64Args &a, cudaStrea
     const Variant &v = variant();
     dim3 g = stage64_grid(a.phys.npx, a.phys.npy);
     int which = (order == 2) ? (stage == 0 ? 0 : 1) : 2;
+    if (a.phys.rk == 0) which = (order == 2) ? 3 : 4;  // MUSCL-Hancock: one stage
     v.k[which]<<<g, v.nthr, v.smem, st>>>(a);
     return cudaGetLastError();
 }

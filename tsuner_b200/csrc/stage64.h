@@ -45,7 +45,8 @@ struct Stage64Args {
     CUtensorMap tmM;  // the uint8 mask [npy][pitch] (box origin x0 - 16)
     int tma;
     double *bufA;           // U^n at step entry (and U^{n+1} at exit, order 2)
-    double *bufB;           // U* (order 2) / ping-pong partner (order 1)
+    double *bufB;           // U* (order 2) / ping-pong partner (order 1, MUSCL-Hancock)
+    double *bufK;           // MUSCL-Hancock: the unfiltered working state carried between steps
     const unsigned char *mask;
     const double *CC;
     const double *tCC;
