@@ -210,6 +210,49 @@ int tsu_last_step_launches(TsuSolver *s, long *launches);
 /* Device pointer of the current state (plane-major, row pitch in elements). */
 int tsu_state_device(TsuSolver *s, void **ptr, long *pitch_elems, long *plane_elems,
                      int *elem_bytes);
+/* ---------------- row slabs of one grid (multi-GPU) ----------------
+ * No counterpart in the reference, which runs one grid on one GPU
+ * (GPU/main_TSUNER.cu:55).  A grid of p->npy rows is split into row slabs,
+ * one per GPU (one process per GPU); a slab owns global rows [j0, j1) and
+ * stores two ghost rows on each side that has a neighbour (every side of a
+ * periodic grid).  The same fused stage kernels run on the owned rows; the
+ * grid's own boundaries (walls, free, the CC series) apply only where a slab
+ * has no neighbour, and the series segments and the dt's float rounding use
+ * the whole grid.  A step is, per RK stage k: the ghost rows of the buffer
+ * the stage reads (k == 0: buffer 0, the state the step starts from;
+ * k == 1: buffer 1, the intermediate state) are exchanged with the
+ * neighbours (tsu_slab_pack -> transport -> tsu_slab_unpack), then
+ * tsu_slab_stage(k); after the last stage the slabs' dt values are reduced
+ * to their minimum (tsu_get_dt_device -> MIN all-reduce -> tsu_set_dt_device)
+ * -- the grid's dt, since each slab rounds its minimum as the whole grid's.
+ * The mask's ghost rows (buffer 2) are exchanged once after tsu_set_mask,
+ * and the dt once after tsu_reset.  FP64 plain form, order 2, RK2 only.
+ * tsu_set_state / set_mask / get_state / get_extrema take and return the
+ * owned rows ([j1 - j0][npx] planes); the boundary series is the whole
+ * grid's.  tsu_step / tsu_run_until refuse a slab.  tsuner_b200/slabs.py
+ * drives slabs over torch.distributed (NCCL send/recv of the ghost rows into
+ * the neighbours' local buffers, no peer loads). */
+int tsu_slab_create(TsuSolver **out, const SimParams *p, const TsuSwitches *sw, int j0, int j1, int device);
+int tsu_slab_info(TsuSolver *s, int *j0, int *rows, int *ghost_south, int *ghost_north);
+/* bytes of one side's message of buffer `which` (0, 1: 5 planes x 2 rows x
+ * npx doubles; 2: the mask, 2 rows x npx bytes) */
+int tsu_slab_halo_bytes(TsuSolver *s, int which, size_t *bytes);
+/* side 0 = south, 1 = north.  pack: the two owned rows next to `side` into
+ * the device buffer d_dst ([planes][2][npx], contiguous); unpack: d_src into
+ * the two ghost rows beyond `side`.  Both enqueue on the solver's stream. */
+int tsu_slab_pack(TsuSolver *s, int which, int side, void *d_dst);
+int tsu_slab_unpack(TsuSolver *s, int which, int side, const void *d_src);
+/* enqueues RK stage k (0 or 1) of the current step on the owned rows */
+int tsu_slab_stage(TsuSolver *s, int k);
+/* the next step's dt to / from one device double (stream-ordered copies) */
+int tsu_get_dt_device(TsuSolver *s, double *d_dt);
+int tsu_set_dt_device(TsuSolver *s, const double *d_dt);
+/* issue all further work of the solver on `stream` (a cudaStream_t; NULL is
+ * CUDA's legacy default stream), e.g. the stream a communication library
+ * uses, so that kernels, copies and messages stay ordered; synchronises the
+ * previous stream first */
+int tsu_set_stream(TsuSolver *s, void *stream);
+
 /* ---------------- batched ensemble (FP32 form) ----------------
  * No counterpart in the reference (single grid only).  nmembers grids of
  * any sizes (params[i]) with their own switches (sw[i]: precision must be 1

@@ -46,6 +46,13 @@ def lib():
         L.orc_run.restype = C.c_long
         L.orc_init_extrema.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_max_threads.restype = C.c_int
+        L.orc_slab_stage.argtypes = [C.POINTER(SimParams), C.POINTER(TsuSwitches), C.c_void_p] + [C.c_int] * 5 + \
+            [C.c_void_p] * 6 + [C.c_ulong, C.c_double, C.c_double, C.c_int]
+        L.orc_slab_stage.restype = C.c_int
+        L.orc_slab_dt.argtypes = [C.POINTER(SimParams), C.POINTER(TsuSwitches)] + [C.c_int] * 4 + [C.c_void_p]
+        L.orc_slab_dt.restype = C.c_double
+        L.orc_slab_extrema.argtypes = [C.POINTER(SimParams)] + [C.c_int] * 4 + [C.c_void_p] * 4
+        L.orc_slab_extrema.restype = None
         _LIB = L
     return _LIB
 
@@ -102,6 +109,114 @@ class OracleRun:
             raise RuntimeError("oracle run failed (%d)" % n)
         self.steps += n
         return n
+
+
+class OracleSlab:
+    """A row slab stepped by the oracle on the host: the compute backend that
+    the CPU tests of tsuner_b200.slabs.SlabGroup put in place of the device
+    (same calls as DeviceSlab; messages are CPU torch tensors, so a gloo
+    group carries them).  It keeps the reference's three state arrays V, V0,
+    Vk for the stored rows; both state buffers of the device (the state a
+    step starts from, the intermediate RK state) are V here, as in the
+    reference, whose V holds whichever state the next stage reads."""
+
+    def __init__(self, p, sw, j0, j1, device=None, kconsts=None):
+        import torch
+        self.torch = torch
+        self.p, self.sw, self.j0, self.j1, self.k = p, sw, j0, j1, kconsts
+        periodic = sw.wbc == 2
+        self.gs = 2 if (j0 > 0 or periodic) else 0
+        self.gn = 2 if (j1 < p.npy or periodic) else 0
+        self.n = j1 - j0
+        nst = self.gs + self.n + self.gn
+        self.V = np.zeros((5, nst, p.npx))
+        self.V0 = np.zeros_like(self.V)
+        self.Vk = np.zeros_like(self.V)
+        self.mask = np.ones((nst, p.npx), np.int32)
+        self.ext = [np.full((nst, p.npx), -1e30) for _ in range(3)]
+        self.CC = self.tCC = None
+        self.timeCC = 0
+        self.t, self.dt, self.dt_local, self.steps = 0.0, -1.0, -1.0, 0
+        self._recv = {}
+        for which in (0, 1, 2):
+            planes = 1 if which == 2 else 5
+            for side in (0, 1):
+                self._recv[which, side] = torch.empty(planes * 2 * p.npx,
+                                                      dtype=torch.uint8 if which == 2 else torch.float64)
+
+    def _rows(self, side, ghost):
+        if ghost:
+            return slice(0, 2) if side == 0 else slice(self.gs + self.n, self.gs + self.n + 2)
+        return slice(self.gs, self.gs + 2) if side == 0 else slice(self.gs + self.n - 2, self.gs + self.n)
+
+    def _slab_args(self):
+        return (self.j0, self.j1, self.gs, self.gn)
+
+    def set_state(self, V):
+        self.V[:, self.gs:self.gs + self.n] = V
+
+    def set_mask(self, mask):
+        self.mask[self.gs:self.gs + self.n] = 1 if mask is None else mask
+
+    def set_boundary_series(self, CC, tCC):
+        self.CC = np.ascontiguousarray(CC, np.float64)
+        self.tCC = np.ascontiguousarray(tCC, np.float64)
+        self.timeCC = len(self.tCC)
+
+    def reset(self):
+        self.t, self.steps = 0.0, 0
+        for e in self.ext:
+            e[:] = -1e30
+        self.V0[:] = self.V
+        self.Vk[:] = self.V
+        self.dt_local = lib().orc_slab_dt(C.byref(self.p), C.byref(self.sw), *self._slab_args(), _ptr(self.V))
+
+    def stage(self, k):
+        kk = None if self.k is None else C.byref(self.k)
+        rc = lib().orc_slab_stage(C.byref(self.p), C.byref(self.sw), kk, *self._slab_args(), k, _ptr(self.V),
+                                  _ptr(self.V0), _ptr(self.Vk), _ptr(self.mask), _ptr(self.CC), _ptr(self.tCC),
+                                  self.timeCC, self.t, self.dt, 0)
+        if rc:
+            raise RuntimeError("oracle slab stage failed (%d)" % rc)
+        if k == self.sw.order - 1:  # the end of the step (GPU/main_TSUNER.cu:185-192)
+            self.t += self.dt
+            self.steps += 1
+            lib().orc_slab_extrema(C.byref(self.p), *self._slab_args(), _ptr(self.V), *[_ptr(e) for e in self.ext])
+            self.dt_local = lib().orc_slab_dt(C.byref(self.p), C.byref(self.sw), *self._slab_args(), _ptr(self.V))
+
+    def pack(self, which, side):
+        rows = self._rows(side, ghost=False)
+        src = self.mask[rows].astype(np.uint8) if which == 2 else self.V[:, rows]
+        return self.torch.from_numpy(np.ascontiguousarray(src).reshape(-1).copy())
+
+    def recv_buffer(self, which, side):
+        return self._recv[which, side]
+
+    def unpack(self, which, side):
+        rows = self._rows(side, ghost=True)
+        buf = self._recv[which, side].numpy()
+        if which == 2:
+            self.mask[rows] = buf.reshape(2, self.p.npx)
+        else:
+            self.V[:, rows] = buf.reshape(5, 2, self.p.npx)
+
+    def dt_buffer(self):
+        return self.torch.tensor([self.dt_local], dtype=self.torch.float64)
+
+    def set_dt(self, d):
+        self.dt = float(d[0])
+
+    def sync(self):
+        pass
+
+    def state(self):
+        return self.V[:, self.gs:self.gs + self.n].copy()
+
+    def extrema(self):
+        return tuple(e[self.gs:self.gs + self.n].copy() for e in self.ext)
+
+    def time(self):
+        return self.t, self.dt, self.steps
 
 
 # ---------------------------------------------------------------- reference

@@ -252,28 +252,41 @@ static void interp_time(const double *CC, const double *tCC, double t, int npx, 
     *hc1 = 0.0;
 }
 
+/* Arrays of stored rows.  A whole grid stores its ny rows.  A row slab of
+ * a decomposed grid (not a reference feature: the reference runs one grid on
+ * one GPU) owns global rows [j0, j1) and also stores gs / gn ghost rows below
+ * / above them, copies of its neighbours' edge rows: stored row r is global
+ * row j0 - gs + r, where rows below 0 or from ny up stand for the wrapped
+ * rows of a periodic grid.  Every array is [5][stored rows][npx]. */
 typedef struct {
-    long nvol;
+    long nvol;                         /* cells per stored plane */
     double *V, *V0, *Vk;               /* 5*nvol each */
     double *rL, *rR, *rD, *rU;         /* 5*nvol each */
     double *FL, *FR, *FD, *FU;         /* 5*nvol each */
     double *dtv;                       /* nvol */
+    int j0, j1, gs, gn, ny;            /* owned rows, ghost rows, global rows */
 } Bufs;
 
-/* reconstructor, GPU/Reconstructor.cu:90-356 (RK == 1 paths) including
- * friction (:33-55, Chezy) and erosion_deposition (:57-88). */
+static inline long rowpos(const Bufs *B, int npx, int j) { return (long)(j - (B->j0 - B->gs)) * npx; }
+
+/* reconstructor, GPU/Reconstructor.cu:90-356 including friction (:33-55)
+ * and erosion_deposition (:57-88).  Faces are built for the owned rows and,
+ * in a slab, for the ghost row next to them (the far side of the slab's
+ * edge); the working state Vk changes only in owned rows. */
 static void reconstruct(const Ctx *C, Bufs *B, double dT, double inv_dx, double inv_dy)
 {
     const SimParams *p = &C->p;
-    const int npx = p->npx, npy = p->npy;
+    const int npx = p->npx, ny = B->ny;
     const long nvol = B->nvol;
     double *V = B->V, *Vk = B->Vk, *V0 = B->V0;
     double *rL = B->rL, *rR = B->rR, *rD = B->rD, *rU = B->rU;
     const int periodic = (C->sw.wbc == 2);
+    const int jr0 = B->j0 - (B->gs ? 1 : 0), jr1 = B->j1 + (B->gn ? 1 : 0);
 #pragma omp parallel for schedule(static)
-    for (int j = 0; j < npy; j++) {
+    for (int j = jr0; j < jr1; j++) {
+        const int owned = (j >= B->j0 && j < B->j1);
         for (int i = 0; i < npx; i++) {
-            long pos = (long)j * npx + i;
+            long pos = rowpos(B, npx, j) + i;
             if (C->sw.order == 1) {
                 for (int f = 0; f < 5; f++)
                     rL[f * nvol + pos] = rR[f * nvol + pos] = rU[f * nvol + pos] = rD[f * nvol + pos] = V[f * nvol + pos];
@@ -288,7 +301,7 @@ static void reconstruct(const Ctx *C, Bufs *B, double dT, double inv_dx, double 
                     if (i == 0) im = npx - 1;
                     if (i == npx - 1) ip = 0;
                 }
-                long pl = (long)j * npx + im, pr = (long)j * npx + ip;
+                long pl = rowpos(B, npx, j) + im, pr = rowpos(B, npx, j) + ip;
                 double hl = V[pl], Hl = V[3 * nvol + pl], cl = V[4 * nvol + pl] / (hl + EPSILON_);
                 double hr = V[pr], Hr = V[3 * nvol + pr], cr = V[4 * nvol + pr] / (hr + EPSILON_);
                 double dta = dT * inv_dx;
@@ -322,17 +335,27 @@ static void reconstruct(const Ctx *C, Bufs *B, double dT, double inv_dx, double 
                 du = avg(dl, dr);
                 rL[4 * nvol + pos] = (ci - 0.5 * du) * rL[pos];
                 rR[4 * nvol + pos] = (ci + 0.5 * du) * rR[pos];
-                Vk[1 * nvol + pos] -= dta * G_ * hi * deta;
+                if (owned) Vk[1 * nvol + pos] -= dta * G_ * hi * deta;
                 const double Tpx = G_ * hi * deta; /* :199-201, used by RK == 0 */
 
-                /* y direction (:207-274) */
-                int jm = j - 1 * (j > 0), jp = j + 1 * (j < npy - 1);
-                if (periodic) {
-                    if (j == 0) jm = npy - 1;
-                    if (j == npy - 1) jp = 0;
+                /* y direction (:207-274): the stored neighbour row where there
+                 * is one (a slab's ghost rows), else the reference's clamp or
+                 * periodic wrap at the grid's own edge */
+                int jm, jp;
+                if (j - 1 >= B->j0 - B->gs) {
+                    jm = j - 1;
+                } else {
+                    jm = j - 1 * (j > 0);
+                    if (periodic && j == 0) jm = ny - 1;
                 }
-                pl = (long)jm * npx + i;
-                pr = (long)jp * npx + i;
+                if (j + 1 < B->j1 + B->gn) {
+                    jp = j + 1;
+                } else {
+                    jp = j + 1 * (j < ny - 1);
+                    if (periodic && j == ny - 1) jp = 0;
+                }
+                pl = rowpos(B, npx, jm) + i;
+                pr = rowpos(B, npx, jp) + i;
                 hl = V[pl]; Hl = V[3 * nvol + pl]; cl = V[4 * nvol + pl] / (hl + EPSILON_);
                 hr = V[pr]; Hr = V[3 * nvol + pr]; cr = V[4 * nvol + pr] / (hr + EPSILON_);
                 dta = dT * inv_dy;
@@ -365,7 +388,7 @@ static void reconstruct(const Ctx *C, Bufs *B, double dT, double inv_dx, double 
                 du = avg(dl, dr);
                 rD[4 * nvol + pos] = (ci - 0.5 * du) * rD[pos];
                 rU[4 * nvol + pos] = (ci + 0.5 * du) * rU[pos];
-                Vk[2 * nvol + pos] -= dta * G_ * hi * deta;
+                if (owned) Vk[2 * nvol + pos] -= dta * G_ * hi * deta;
                 const double Tpy = G_ * hi * deta; /* :276-278 */
 
                 if (C->sw.rk == 0) {
@@ -411,7 +434,7 @@ static void reconstruct(const Ctx *C, Bufs *B, double dT, double inv_dx, double 
             }
             /* friction, :33-55: Chezy (Manning == 0) or the reference's
              * unfinished Manning branch (:47-50), which multiplies by c */
-            {
+            if (owned) {
                 double h = V0[pos], ux, uy;
                 vel(h, V0[1 * nvol + pos], V0[2 * nvol + pos], &ux, &uy);
                 double modu = sqrt(ux * ux + uy * uy);
@@ -426,7 +449,7 @@ static void reconstruct(const Ctx *C, Bufs *B, double dT, double inv_dx, double 
                 }
             }
             /* erosion_deposition, :57-88, calculate_erosion/deposition SedFlux.cuh:51-99 */
-            {
+            if (owned) {
                 double h = V0[pos], ux, uy;
                 double c = V0[4 * nvol + pos] / (h + p->epsilon_h);
                 vel(h, V0[1 * nvol + pos], V0[2 * nvol + pos], &ux, &uy);
@@ -472,7 +495,11 @@ static void ghost(const Ctx *C, const double *CC, const double *tCC, unsigned lo
     }
 }
 
-/* VolumeSolver, GPU/VolumeSolver.cu:217-408 */
+/* VolumeSolver, GPU/VolumeSolver.cu:217-408.  In a slab the edges of the
+ * owned rows are evaluated: the horizontal edge between an owned row and a
+ * ghost row is an interior edge (or, at a periodic grid's south / north
+ * edge, the periodic seam of :352-367,378-387), and only the owned side's
+ * fluctuation is used. */
 static void volume_solver(const Ctx *C, Bufs *B, const int *fixH, double t, const double *CC,
                           const double *tCC, unsigned long timeCC)
 {
@@ -482,12 +509,12 @@ static void volume_solver(const Ctx *C, Bufs *B, const int *fixH, double t, cons
     double *FL = B->FL, *FR = B->FR, *FD = B->FD, *FU = B->FU;
     const int periodic = (C->sw.wbc == 2);
 #pragma omp parallel for schedule(static)
-    for (int j = 0; j <= npy; j++) {
+    for (int j = B->j0; j <= B->j1; j++) {
         for (int i = 0; i <= npx; i++) {
             double Dm[5], Dp[5];
             double h0, h1, zb0, zb1, hc0, hc1, q0x, q0y, q1x, q1y;
-            if (j < npy) { /* vertical edges (:228-317) */
-                long pos0 = i - 1 + (long)j * npx, pos1 = i + (long)j * npx;
+            if (j < B->j1) { /* vertical edges (:228-317) */
+                long pos0 = i - 1 + rowpos(B, npx, j), pos1 = i + rowpos(B, npx, j);
                 if (i == 0) {
                     if (!periodic) {
                         pos0 = pos1;
@@ -501,7 +528,7 @@ static void volume_solver(const Ctx *C, Bufs *B, const int *fixH, double t, cons
                     h0 = rR[pos0]; q0x = rR[nvol + pos0]; q0y = rR[2 * nvol + pos0];
                     zb0 = rR[3 * nvol + pos0]; hc0 = rR[4 * nvol + pos0];
                     if (periodic) {
-                        pos1 = (long)j * npx;
+                        pos1 = rowpos(B, npx, j);
                         h1 = rL[pos1]; q1x = rL[nvol + pos1]; q1y = rL[2 * nvol + pos1];
                         zb1 = rL[3 * nvol + pos1]; hc1 = rL[4 * nvol + pos1];
                         if (C->sw.read_files) {
@@ -527,8 +554,8 @@ static void volume_solver(const Ctx *C, Bufs *B, const int *fixH, double t, cons
                 }
             }
             if (i < npx) { /* horizontal edges (:319-406) */
-                long pos0 = i + (long)(j - 1) * npx, pos1 = i + (long)j * npx;
-                if (j == 0) {
+                long pos0 = i + rowpos(B, npx, j - 1), pos1 = i + rowpos(B, npx, j);
+                if (j == 0 && B->gs == 0) {
                     if (!periodic) {
                         pos0 = pos1;
                         h1 = h0 = rD[pos0]; q1x = q0x = rD[nvol + pos0]; q1y = q0y = rD[2 * nvol + pos0];
@@ -537,11 +564,11 @@ static void volume_solver(const Ctx *C, Bufs *B, const int *fixH, double t, cons
                         riemann(C, h0, zb0, q0x, q0y, hc0, h1, zb1, q1x, q1y, hc1, 0, -1, fixH[pos0], Dm, Dp);
                         put(FD, nvol, pos0, Dm);
                     }
-                } else if (j == npy) {
+                } else if (j == npy && B->gn == 0) {
                     h0 = rU[pos0]; q0x = rU[nvol + pos0]; q0y = rU[2 * nvol + pos0];
                     zb0 = rU[3 * nvol + pos0]; hc0 = rU[4 * nvol + pos0];
                     if (periodic) {
-                        pos1 = i;
+                        pos1 = i + rowpos(B, npx, 0);
                         h1 = rD[pos1]; q1x = rD[nvol + pos1]; q1y = rD[2 * nvol + pos1];
                         zb1 = rD[3 * nvol + pos1]; hc1 = rD[4 * nvol + pos1];
                         if (C->sw.read_files) {
@@ -556,6 +583,21 @@ static void volume_solver(const Ctx *C, Bufs *B, const int *fixH, double t, cons
                     riemann(C, h0, zb0, q0x, q0y, hc0, h1, zb1, q1x, q1y, hc1, 0, 1, fixH[pos0], Dm, Dp);
                     put(FU, nvol, pos0, Dm);
                     if (periodic) put(FD, nvol, pos1, Dp);
+                } else if (periodic && (j == 0 || j == npy)) {
+                    /* a slab's side of the periodic seam: the wrapped row is
+                     * its ghost row; the same edge as the j == npy case above */
+                    h0 = rU[pos0]; q0x = rU[nvol + pos0]; q0y = rU[2 * nvol + pos0];
+                    zb0 = rU[3 * nvol + pos0]; hc0 = rU[4 * nvol + pos0];
+                    h1 = rD[pos1]; q1x = rD[nvol + pos1]; q1y = rD[2 * nvol + pos1];
+                    zb1 = rD[3 * nvol + pos1]; hc1 = rD[4 * nvol + pos1];
+                    if (C->sw.read_files) {
+                        if (t < tCC[timeCC - 2])
+                            interp_time(CC, tCC, t, npx, npy, npx + npy + i, &h1, &zb1, &q1x, &q1y, &hc1);
+                        else q1y = -q0y;
+                    }
+                    riemann(C, h0, zb0, q0x, q0y, hc0, h1, zb1, q1x, q1y, hc1, 0, 1, fixH[pos0], Dm, Dp);
+                    put(FU, nvol, pos0, Dm);
+                    put(FD, nvol, pos1, Dp);
                 } else {
                     h0 = rU[pos0]; q0x = rU[nvol + pos0]; q0y = rU[2 * nvol + pos0];
                     zb0 = rU[3 * nvol + pos0]; hc0 = rU[4 * nvol + pos0];
@@ -576,10 +618,12 @@ static void volume_solver(const Ctx *C, Bufs *B, const int *fixH, double t, cons
 static void update(const Ctx *C, Bufs *B, int k, double invx, double invy)
 {
     const long nvol = B->nvol;
+    const int npx = C->p.npx, nown = B->j1 - B->j0;
     double *Vk = B->Vk, *V0 = B->V0, *V = B->V;
     const double *FL = B->FL, *FR = B->FR, *FD = B->FD, *FU = B->FU;
 #pragma omp parallel for schedule(static)
-    for (long pos = 0; pos < nvol; pos++) {
+    for (long c = 0; c < (long)nown * npx; c++) { /* the owned cells */
+        const long pos = rowpos(B, npx, B->j0 + (int)(c / npx)) + c % npx;
         for (int f = 0; f < 5; f++) {
             long q = f * nvol + pos;
             Vk[q] -= invx * (FL[q] + FR[q]) + invy * (FD[q] + FU[q]);
@@ -612,9 +656,11 @@ static void update(const Ctx *C, Bufs *B, int k, double invx, double invy)
  * (GPU/Reduction_kernel_min.cu:155-196): for n > 4096 every device compare is
  * fminf on doubles, so the result is the float-rounded minimum; for n <= 4096
  * an exact host minimum.  Both are capped by the 1e30 start value. */
-static double get_dt(const Ctx *C, const double *V, long nvol)
+static double get_dt(const Ctx *C, const double *V, const Bufs *B)
 {
     const SimParams *p = &C->p;
+    const long nvol = B->nvol;
+    const int npx = p->npx, nown = B->j1 - B->j0;
     double m = INFINITY;
     int any = 0;
 #pragma omp parallel
@@ -622,7 +668,8 @@ static double get_dt(const Ctx *C, const double *V, long nvol)
         double lm = INFINITY;
         int la = 0;
 #pragma omp for schedule(static)
-        for (long pos = 0; pos < nvol; pos++) {
+        for (long c = 0; c < (long)nown * npx; c++) { /* the owned cells */
+            const long pos = rowpos(B, npx, B->j0 + (int)(c / npx)) + c % npx;
             double ux, uy;
             double h = V[pos];
             vel(h, V[nvol + pos], V[2 * nvol + pos], &ux, &uy);
@@ -638,7 +685,10 @@ static double get_dt(const Ctx *C, const double *V, long nvol)
         }
     }
     if (!any) return 1e30;
-    if (nvol > 4096) m = (double)(float)m;
+    /* the rounding follows the whole grid's cell count (a slab's minimum is
+     * rounded as the grid's would be; rounding is monotonic, so the minimum
+     * over slabs of their rounded minima is the grid's) */
+    if ((long)npx * B->ny > 4096) m = (double)(float)m;
     if (!(m < 1e30)) m = 1e30;
     return m;
 }
@@ -652,7 +702,12 @@ double orc_initial_dt(const SimParams *p, const TsuSwitches *sw, const double *V
     C.p = *p;
     C.sw = *sw;
     orc_consts(p, &C.k);
-    return get_dt(&C, V, (long)p->npx * p->npy);
+    Bufs B;
+    memset(&B, 0, sizeof(B));
+    B.nvol = (long)p->npx * p->npy;
+    B.j0 = 0;
+    B.j1 = B.ny = p->npy;
+    return get_dt(&C, V, &B);
 }
 
 /*
@@ -684,6 +739,9 @@ long orc_run(const SimParams *p, const TsuSwitches *sw, const TsuConsts *kin, do
     if (sw->read_files && timeCC < 2) return -2;
     Bufs B;
     B.nvol = (long)p->npx * p->npy;
+    B.j0 = 0;
+    B.j1 = B.ny = p->npy;
+    B.gs = B.gn = 0;
     size_t n5 = (size_t)5 * B.nvol;
     double *mem = (double *)malloc(sizeof(double) * (n5 * 10 + B.nvol));
     if (!mem) return -1;
@@ -698,7 +756,7 @@ long orc_run(const SimParams *p, const TsuSwitches *sw, const TsuConsts *kin, do
     memcpy(B.Vk, Vk_io ? Vk_io : V, sizeof(double) * n5);
     double inv_dx = 1.0 / p->dx, inv_dy = 1.0 / p->dy;
     double dT = *dt;
-    if (dT < 0) dT = get_dt(&C, V, B.nvol);
+    if (dT < 0) dT = get_dt(&C, V, &B);
     double ct = *t;
     long it = 0;
     /* GPU/main_TSUNER.cu:169-174: `order` RK stages, or one MUSCL-Hancock stage */
@@ -722,7 +780,7 @@ long orc_run(const SimParams *p, const TsuSwitches *sw, const TsuConsts *kin, do
                 if (eta_max && h > eps_h) eta_max[pos] = dmax(eta_max[pos], h - H);
             }
         }
-        dT = get_dt(&C, V, B.nvol);
+        dT = get_dt(&C, V, &B);
         it++;
     }
     *t = ct;
@@ -730,6 +788,89 @@ long orc_run(const SimParams *p, const TsuSwitches *sw, const TsuConsts *kin, do
     if (Vk_io) memcpy(Vk_io, B.Vk, sizeof(double) * n5);
     free(mem);
     return it;
+}
+
+/* ---- row slabs of a decomposed grid (the multi-GPU form; no reference
+ * counterpart).  p is the WHOLE grid; the slab owns global rows [j0, j1) and
+ * stores gs / gn ghost rows below / above them, so every array is
+ * [5][gs + (j1 - j0) + gn][npx] (fixH [stored rows][npx]).  The caller fills
+ * the ghost rows of V (the state the stage reads) and of fixH from the
+ * neighbouring slabs before each stage. */
+static void slab_bufs(const SimParams *p, int j0, int j1, int gs, int gn, Bufs *B)
+{
+    memset(B, 0, sizeof(*B));
+    B->j0 = j0;
+    B->j1 = j1;
+    B->gs = gs;
+    B->gn = gn;
+    B->ny = p->npy;
+    B->nvol = (long)p->npx * (gs + (j1 - j0) + gn);
+}
+
+/* Stage k of a step (GPU/main_TSUNER.cu:169-183: reconstructor,
+ * VolumeSolver, states_updater) for the owned rows at time t with step dT.
+ * V, V0, Vk are the reference's three state arrays for the stored rows.
+ * Returns 0, or -1 on allocation failure. */
+int orc_slab_stage(const SimParams *p, const TsuSwitches *sw, const TsuConsts *kin, int j0, int j1, int gs, int gn,
+                   int k, double *V, double *V0, double *Vk, const int *fixH, const double *CC, const double *tCC,
+                   unsigned long timeCC, double t, double dT, int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    Ctx C;
+    C.p = *p;
+    C.sw = *sw;
+    if (kin) C.k = *kin;
+    else orc_consts(p, &C.k);
+    Bufs B;
+    slab_bufs(p, j0, j1, gs, gn, &B);
+    const size_t n5 = (size_t)5 * B.nvol;
+    double *mem = (double *)calloc(n5 * 8, sizeof(double));
+    if (!mem) return -1;
+    B.V = V;
+    B.V0 = V0;
+    B.Vk = Vk;
+    B.rL = mem; B.rR = mem + n5; B.rD = mem + 2 * n5; B.rU = mem + 3 * n5;
+    B.FL = mem + 4 * n5; B.FR = mem + 5 * n5; B.FD = mem + 6 * n5; B.FU = mem + 7 * n5;
+    const double inv_dx = 1.0 / p->dx, inv_dy = 1.0 / p->dy;
+    reconstruct(&C, &B, dT, inv_dx, inv_dy);
+    volume_solver(&C, &B, fixH, t, CC, tCC, timeCC);
+    update(&C, &B, k, dT * inv_dx, dT * inv_dy);
+    free(mem);
+    return 0;
+}
+
+/* GetDeltaT + MinReduction over the owned rows, rounded as for the whole
+ * grid: the minimum over all slabs of these values is the grid's dt. */
+double orc_slab_dt(const SimParams *p, const TsuSwitches *sw, int j0, int j1, int gs, int gn, const double *V)
+{
+    Ctx C;
+    C.p = *p;
+    C.sw = *sw;
+    orc_consts(p, &C.k);
+    Bufs B;
+    slab_bufs(p, j0, j1, gs, gn, &B);
+    return get_dt(&C, V, &B);
+}
+
+/* hmax / bmin / eta_max_calculator (GPU/Volume_kernel.cu:79-110) on the owned
+ * rows; the extrema arrays are [stored rows][npx] like V's planes. */
+void orc_slab_extrema(const SimParams *p, int j0, int j1, int gs, int gn, const double *V, double *hmax,
+                      double *bmin, double *eta_max)
+{
+    Bufs B;
+    slab_bufs(p, j0, j1, gs, gn, &B);
+    const long nvol = B.nvol;
+    const int npx = p->npx;
+    for (int j = j0; j < j1; j++)
+        for (int i = 0; i < npx; i++) {
+            const long pos = rowpos(&B, npx, j) + i;
+            const double h = V[pos], H = V[3 * nvol + pos];
+            if (h > p->epsilon_h) hmax[pos] = dmax(hmax[pos], h);
+            bmin[pos] = dmax(bmin[pos], H);
+            if (h > p->epsilon_h) eta_max[pos] = dmax(eta_max[pos], h - H);
+        }
 }
 
 /* set_inicializacion*, GPU/Volume_kernel.cu:112-137 */

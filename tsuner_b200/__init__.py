@@ -38,6 +38,8 @@ EXPORTS = [
     "tsu_corr_get_weights", "tsu_corr_set_weights", "tsu_corr_train", "tsu_corr_predict", "tsu_corr_bench_conv",
     "tsu_corr_last_train_ms", "tsu_corr_conv3x3", "tsu_corr_conv3x3_wgrad", "tsu_corr_status",
     "tsu_corr_last_error", "tsu_set_wait_limit_ns",
+    "tsu_slab_create", "tsu_slab_info", "tsu_slab_halo_bytes", "tsu_slab_pack", "tsu_slab_unpack", "tsu_slab_stage",
+    "tsu_get_dt_device", "tsu_set_dt_device", "tsu_set_stream",
 ]
 
 _ENS_SIG = {
@@ -130,6 +132,16 @@ def lib():
             "tsu_parse_data_dat": ([C.c_char_p, C.POINTER(SimParams), C.c_char_p, C.c_char_p, C.c_char_p,
                                     C.c_char_p, C.POINTER(C.c_double), C.c_char_p, C.c_size_t], C.c_int),
             "tsu_set_wait_limit_ns": ([C.c_ulonglong], C.c_int),
+            "tsu_slab_create": ([C.POINTER(vp), C.POINTER(SimParams), C.POINTER(TsuSwitches), C.c_int, C.c_int,
+                                 C.c_int], C.c_int),
+            "tsu_slab_info": ([vp] + [C.POINTER(C.c_int)] * 4, C.c_int),
+            "tsu_slab_halo_bytes": ([vp, C.c_int, C.POINTER(C.c_size_t)], C.c_int),
+            "tsu_slab_pack": ([vp, C.c_int, C.c_int, vp], C.c_int),
+            "tsu_slab_unpack": ([vp, C.c_int, C.c_int, vp], C.c_int),
+            "tsu_slab_stage": ([vp, C.c_int], C.c_int),
+            "tsu_get_dt_device": ([vp, vp], C.c_int),
+            "tsu_set_dt_device": ([vp, vp], C.c_int),
+            "tsu_set_stream": ([vp, vp], C.c_int),
             "checkCUDAsupport": ([C.c_int], C.c_int),
             "initializeGPU": ([], None),
         }

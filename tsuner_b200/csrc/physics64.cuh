@@ -31,6 +31,12 @@ struct Phys64 {
     int order, wbc, bedload, suspension, read_files, bedload_law;
     double grass_ag;
     int rk, manning;
+    // Row slab of a decomposed grid: npy is the number of rows this solver
+    // owns, starting at global row j0 of a grid of ny_glob rows; gs / gn
+    // ghost rows (0 or 2) below / above the owned rows are stored in the
+    // state and mask planes and filled by the halo exchange.  A whole grid
+    // has ny_glob = npy, j0 = 0, gs = gn = 0.
+    int ny_glob, j0, gs, gn;
 };
 
 // IEEE quotient and square root with the zero cases answered directly:

@@ -58,17 +58,26 @@ void tsu_set_error_detail(const char *text) { snprintf(g_err, sizeof(g_err), "%s
 int tsu_device_flags(TsuSolver *s, const double *sc) {
     if (sc[SC_ERR] != 0.0) {
         s->ready = false;
+        s->fault = TSU_ERR_CUDA;
         snprintf(g_err, sizeof(g_err), "a bounded device wait for a tile load expired (step %.0f); tsu_reset "
                  "before stepping again", sc[SC_STEPS]);
         return TSU_ERR_CUDA;
     }
     if (sc[SC_NAN] != 0.0) {
         s->ready = false;
+        s->fault = TSU_ERR_NONFINITE;
         snprintf(g_err, sizeof(g_err), "the state holds a NaN or an infinite value (detected at step %.0f)",
                  sc[SC_STEPS]);
         return TSU_ERR_NONFINITE;
     }
     return TSU_OK;
+}
+
+// a solver whose kernels reported an error steps again only after tsu_reset
+static int fault_refuses(TsuSolver *s, const char *what) {
+    snprintf(g_err, sizeof(g_err), "%s: the last steps reported %s; tsu_reset (after tsu_set_state for a "
+             "non-finite state) before stepping again", what, tsu_strerror(s->fault));
+    return TSU_ERR_INVALID;
 }
 
 static int device_flags(TsuSolver *s) {
@@ -139,7 +148,7 @@ static void free_all(TsuSolver *s) {
     cudaFree(s->dconsts);
     if (s->e0) cudaEventDestroy(s->e0);
     if (s->e1) cudaEventDestroy(s->e1);
-    if (s->st) cudaStreamDestroy(s->st);
+    if (s->own_st) cudaStreamDestroy(s->own_st);
 }
 
 static void fill_phys(TsuSolver *s) {
@@ -170,6 +179,10 @@ static void fill_phys(TsuSolver *s) {
     P.grass_ag = sw->grass_ag;
     P.rk = sw->rk;
     P.manning = sw->manning;
+    P.ny_glob = s->ny_glob;
+    P.j0 = s->j0;
+    P.gs = s->gs;
+    P.gn = s->gn;
     Phys32 &Q = s->phys32;
     Q.eta0 = sw->eta0;
     Q.eta0f = (float)sw->eta0;
@@ -204,10 +217,13 @@ static void fill_phys(TsuSolver *s) {
     Q.grass_ag = (float)sw->grass_ag;
 }
 
-extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches *sw, int device) {
+// A solver for global rows [j0, j1) of the grid p (the whole grid: 0, npy),
+// storing gs / gn ghost rows below / above them.
+static int create_solver(TsuSolver **out, const SimParams *pg, const TsuSwitches *sw, int device, int j0, int j1,
+                         int gs, int gn) {
     if (!out) return TSU_ERR_INVALID;
     *out = nullptr;
-    int rc = validate(p, sw);
+    int rc = validate(pg, sw);
     if (rc) {
         snprintf(g_err, sizeof(g_err), "invalid parameters or switches");
         return rc;
@@ -222,13 +238,21 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
     CK(cudaSetDevice(device));
     TsuSolver *s = new (std::nothrow) TsuSolver();
     if (!s) return TSU_ERR_HOST_OOM;
-    s->p = *p;
-    s->p.nvol = p->npx * p->npy;
+    s->p = *pg;
+    s->p.npy = j1 - j0;  // the owned rows
+    s->p.nvol = pg->npx * s->p.npy;
+    s->slab = (j0 != 0 || j1 != pg->npy || gs || gn);
+    s->j0 = j0;
+    s->gs = gs;
+    s->gn = gn;
+    s->ny_glob = pg->npy;
+    const SimParams *p = &s->p;
     s->sw = *sw;
     s->device = device;
     s->fp32 = (sw->precision == 1);
     s->pitch = ((long long)p->npx + 31) / 32 * 32;
-    s->plane = s->pitch * p->npy;
+    const int nstore = gs + p->npy + gn;
+    s->plane = s->pitch * nstore;
     const size_t pl = (size_t)s->plane * s->elem();
     cudaError_t e = cudaSuccess;
 #define AL(ptr, bytes) \
@@ -246,7 +270,8 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
     AL(s->ticket, sizeof(unsigned));
     AL(s->dconsts, sizeof(TsuConsts));
 #undef AL
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own_st, cudaStreamNonBlocking);
+    s->st = s->own_st;
     if (e == cudaSuccess) e = cudaEventCreate(&s->e0);
     if (e == cudaSuccess) e = cudaEventCreate(&s->e1);
     if (e == cudaSuccess) e = s->fp32 ? stage32_prepare() : stage64_prepare();
@@ -270,8 +295,9 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
             s->tmB = t32.b;
             s->tmM = t32.m;
         } else {
+            // the maps cover every stored row (ghost rows included)
             s->tma = stage64_tma_maps((const double *)s->A, (const double *)s->B, s->mask, s->pitch, s->plane, p->npx,
-                                      p->npy, &s->tmA, &s->tmB, &s->tmM);
+                                      nstore, &s->tmA, &s->tmB, &s->tmM);
         }
     }
     if (e != cudaSuccess) {
@@ -283,6 +309,29 @@ extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches
     fill_phys(s);
     *out = s;
     return TSU_OK;
+}
+
+extern "C" int tsu_create(TsuSolver **out, const SimParams *p, const TsuSwitches *sw, int device) {
+    if (!p) return TSU_ERR_INVALID;
+    return create_solver(out, p, sw, device, 0, p->npy, 0, 0);
+}
+
+extern "C" int tsu_slab_create(TsuSolver **out, const SimParams *p, const TsuSwitches *sw, int j0, int j1,
+                               int device) {
+    if (out) *out = nullptr;
+    if (!p || !sw || !out) return TSU_ERR_INVALID;
+    if (j0 < 0 || j1 > p->npy || j1 - j0 < 2 || (j0 == 0 && j1 == p->npy)) {
+        snprintf(g_err, sizeof(g_err), "slab rows [%d, %d) of a %d-row grid: a slab owns at least 2 rows and not "
+                 "the whole grid", j0, j1, p->npy);
+        return TSU_ERR_INVALID;
+    }
+    if (sw->precision != 0 || sw->order != 2 || sw->rk != 1) {
+        snprintf(g_err, sizeof(g_err), "row slabs are built for the FP64 plain form with order 2 and RK2");
+        return TSU_ERR_INVALID;
+    }
+    const bool periodic = (sw->wbc == 2);
+    const int gs = (j0 > 0 || periodic) ? 2 : 0, gn = (j1 < p->npy || periodic) ? 2 : 0;
+    return create_solver(out, p, sw, device, j0, j1, gs, gn);
 }
 
 extern "C" int tsu_destroy(TsuSolver *s) {
@@ -313,10 +362,10 @@ extern "C" int tsu_set_state(TsuSolver *s, const double *h, const double *qx, co
     int n = 0;
     for (int f = 0; f < 5; f++) {
         if (src[f]) {
-            dst[n] = base + f * s->plane;
+            dst[n] = base + f * s->plane + s->own_off();
             from[n++] = src[f];
         } else {
-            CK(cudaMemsetAsync(base + f * s->plane, 0, (size_t)s->plane * sizeof(double), s->st));
+            CK(cudaMemsetAsync(base + f * s->plane, 0, (size_t)s->plane * sizeof(double), s->st));  // ghost rows too
         }
     }
     CK(tsu::planes_h2d(n, dst, s->pitch * sizeof(double), from, s->p.npx * sizeof(double), s->p.npx * sizeof(double),
@@ -355,7 +404,7 @@ extern "C" int tsu_set_mask(TsuSolver *s, const int *fixH) {
             snprintf(g_err, sizeof(g_err), "mask value %d at %lld is not 0 or 1", fixH[bad[q]], bad[q]);
             return TSU_ERR_INVALID;
         }
-    void *dst[1] = {s->mask};
+    void *dst[1] = {s->mask + s->own_off()};
     const void *from[1] = {fixH};
     CK(tsu::planes_h2d(1, dst, s->pitch, from, npx * sizeof(int), npx, npy, s->st,
                        [&](int, size_t r0, size_t nr, unsigned char *out) {
@@ -407,16 +456,19 @@ extern "C" int tsu_set_boundary_series(TsuSolver *s, const double *CC, const dou
 
 Stage64Args TsuSolver::args() const {
     Stage64Args a;
-    a.bufA = (double *)A;
-    a.bufB = (double *)B;
-    a.bufK = (double *)K;
-    a.mask = mask;
+    // the kernels address the owned rows from row 0; a slab's ghost rows
+    // lie below (negative offsets) and above them
+    const long long o = own_off();
+    a.bufA = (double *)A + o;
+    a.bufB = (double *)B + o;
+    a.bufK = K ? (double *)K + o : nullptr;
+    a.mask = mask + o;
     a.CC = CC;
     a.tCC = tCC;
     a.timeCC = timeCC;
-    a.hmax = (double *)hmax;
-    a.bmin = (double *)bmin;
-    a.eta_max = (double *)eta;
+    a.hmax = (double *)hmax + o;
+    a.bmin = (double *)bmin + o;
+    a.eta_max = (double *)eta + o;
     a.scal = scal;
     a.partials = partials;
     a.ticket = ticket;
@@ -465,6 +517,7 @@ extern "C" int tsu_reset(TsuSolver *s) {
     }
     CK(cudaSetDevice(s->device));
     s->ready = false;
+    s->fault = 0;
     const size_t state_bytes = 5 * (size_t)s->plane * s->elem();
     if (s->single_stage()) {
         // the state may sit in B after an odd number of single-stage steps:
@@ -488,7 +541,7 @@ extern "C" int tsu_reset(TsuSolver *s) {
         CK(fill_launch((double *)s->hmax, s->plane, -1e30, s->st));  // GPU/Volume_kernel.cu:112-137
         CK(fill_launch((double *)s->bmin, s->plane, -1e30, s->st));
         CK(fill_launch((double *)s->eta, s->plane, -1e30, s->st));
-        CK(initial_dt_launch((const double *)s->A, s->pitch, s->plane, s->phys, s->partials, s->ticket, s->scal,
+        CK(initial_dt_launch((const double *)s->A + s->own_off(), s->pitch, s->plane, s->phys, s->partials, s->ticket, s->scal,
                              s->st));
     }
     CK(cudaStreamSynchronize(s->st));
@@ -516,8 +569,16 @@ int TsuSolver::launch_steps(long n) {
     return TSU_OK;
 }
 
+static int slab_refuses(TsuSolver *s, const char *what) {
+    snprintf(g_err, sizeof(g_err), "%s: a row slab steps stage by stage (tsu_slab_stage) with its halo exchange "
+             "in between", what);
+    return TSU_ERR_INVALID;
+}
+
 extern "C" int tsu_step(TsuSolver *s, long nsteps) {
     if (!s || nsteps < 0) return TSU_ERR_INVALID;
+    if (s->slab) return slab_refuses(s, "tsu_step");
+    if (s->fault) return fault_refuses(s, "tsu_step");
     if (s->sw.read_files && s->timeCC < 2) {  // e.g. the last series upload failed
         snprintf(g_err, sizeof(g_err), "read_files is set but no boundary series is loaded");
         return TSU_ERR_INVALID;
@@ -559,6 +620,108 @@ extern "C" int tsu_sync(TsuSolver *s) {
     return device_flags(s);
 }
 
+// ------------------------------------------------------------- row slabs
+extern "C" int tsu_set_stream(TsuSolver *s, void *stream) {
+    if (!s) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->st));  // work issued so far completes first
+    s->invalidate_graph();
+    s->st = static_cast<cudaStream_t>(stream);
+    return TSU_OK;
+}
+
+extern "C" int tsu_slab_info(TsuSolver *s, int *j0, int *rows, int *ghost_south, int *ghost_north) {
+    if (!s) return TSU_ERR_INVALID;
+    if (j0) *j0 = s->j0;
+    if (rows) *rows = s->p.npy;
+    if (ghost_south) *ghost_south = s->gs;
+    if (ghost_north) *ghost_north = s->gn;
+    return TSU_OK;
+}
+
+extern "C" int tsu_slab_stage(TsuSolver *s, int k) {
+    if (!s || !s->slab || k < 0 || k >= s->stages()) return TSU_ERR_INVALID;
+    if (s->fault) return fault_refuses(s, "tsu_slab_stage");
+    if (!s->ready) {
+        snprintf(g_err, sizeof(g_err), "tsu_slab_stage: tsu_reset the slab first");
+        return TSU_ERR_INVALID;
+    }
+    if (s->sw.read_files && s->timeCC < 2) {
+        snprintf(g_err, sizeof(g_err), "read_files is set but no boundary series is loaded");
+        return TSU_ERR_INVALID;
+    }
+    CK(cudaSetDevice(s->device));
+    CK(stage64_launch(s->sw.order, k, s->args(), s->st));
+    return TSU_OK;
+}
+
+// which: 0 = buffer A (the state a step starts from), 1 = buffer B (the
+// intermediate RK2 state), 2 = the mask; side: 0 = south, 1 = north
+static int halo_geometry(TsuSolver *s, int which, int side, size_t *elem, int *planes) {
+    if (!s || !s->slab || which < 0 || which > 2 || side < 0 || side > 1 || s->p.npy < 2) return TSU_ERR_INVALID;
+    *elem = (which == 2) ? 1 : s->elem();
+    *planes = (which == 2) ? 1 : 5;
+    return TSU_OK;
+}
+
+extern "C" int tsu_slab_halo_bytes(TsuSolver *s, int which, size_t *bytes) {
+    size_t el;
+    int np;
+    if (!bytes || halo_geometry(s, which, 0, &el, &np)) return TSU_ERR_INVALID;
+    *bytes = (size_t)np * 2 * s->p.npx * el;
+    return TSU_OK;
+}
+
+// the two owned rows next to `side` -> d_dst [planes][2][npx] (contiguous)
+extern "C" int tsu_slab_pack(TsuSolver *s, int which, int side, void *d_dst) {
+    size_t el;
+    int np;
+    if (!d_dst || halo_geometry(s, which, side, &el, &np)) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    char *base = static_cast<char *>(which == 2 ? (void *)s->mask : which == 0 ? s->A : s->B);
+    const long long row = s->gs + (side == 0 ? 0 : s->p.npy - 2);  // stored row of the first one
+    const size_t w = (size_t)s->p.npx * el, sp = (size_t)s->pitch * el;
+    for (int f = 0; f < np; f++)
+        CK(cudaMemcpy2DAsync(static_cast<char *>(d_dst) + (size_t)f * 2 * w, w,
+                             base + ((size_t)f * s->plane + (size_t)row * s->pitch) * el, sp, w, 2,
+                             cudaMemcpyDeviceToDevice, s->st));
+    return TSU_OK;
+}
+
+// d_src [planes][2][npx] -> the two ghost rows beyond `side`
+extern "C" int tsu_slab_unpack(TsuSolver *s, int which, int side, const void *d_src) {
+    size_t el;
+    int np;
+    if (!d_src || halo_geometry(s, which, side, &el, &np)) return TSU_ERR_INVALID;
+    if ((side == 0 && s->gs < 2) || (side == 1 && s->gn < 2)) {
+        snprintf(g_err, sizeof(g_err), "tsu_slab_unpack: the slab has no ghost rows on side %d", side);
+        return TSU_ERR_INVALID;
+    }
+    CK(cudaSetDevice(s->device));
+    char *base = static_cast<char *>(which == 2 ? (void *)s->mask : which == 0 ? s->A : s->B);
+    const long long row = (side == 0) ? 0 : s->gs + s->p.npy;  // stored row of the first ghost row
+    const size_t w = (size_t)s->p.npx * el, sp = (size_t)s->pitch * el;
+    for (int f = 0; f < np; f++)
+        CK(cudaMemcpy2DAsync(base + ((size_t)f * s->plane + (size_t)row * s->pitch) * el, sp,
+                             static_cast<const char *>(d_src) + (size_t)f * 2 * w, w, w, 2, cudaMemcpyDeviceToDevice,
+                             s->st));
+    return TSU_OK;
+}
+
+extern "C" int tsu_get_dt_device(TsuSolver *s, double *d_dt) {
+    if (!s || !d_dt) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    CK(cudaMemcpyAsync(d_dt, s->scal + SC_DT, sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    return TSU_OK;
+}
+
+extern "C" int tsu_set_dt_device(TsuSolver *s, const double *d_dt) {
+    if (!s || !d_dt) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    CK(cudaMemcpyAsync(s->scal + SC_DT, d_dt, sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    return TSU_OK;
+}
+
 extern "C" int tsu_set_wait_limit_ns(unsigned long long ns) {
     if (ns == 0) ns = kDefaultWaitNs;
     CK(set_wait_limit_stage64(ns));
@@ -569,6 +732,8 @@ extern "C" int tsu_set_wait_limit_ns(unsigned long long ns) {
 
 extern "C" int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *steps_done) {
     if (!s || max_steps < 0) return TSU_ERR_INVALID;
+    if (s->slab) return slab_refuses(s, "tsu_run_until");
+    if (s->fault) return fault_refuses(s, "tsu_run_until");
     if (s->sw.read_files && s->timeCC < 2) {  // e.g. the last series upload failed
         snprintf(g_err, sizeof(g_err), "read_files is set but no boundary series is loaded");
         return TSU_ERR_INVALID;
@@ -627,7 +792,7 @@ extern "C" int tsu_get_state(TsuSolver *s, double *V) {
     const void *from[5];
     for (int f = 0; f < 5; f++) {
         dst[f] = V + f * n;
-        from[f] = cur + f * s->plane;
+        from[f] = cur + f * s->plane + s->own_off();
     }
     CK(tsu::planes_d2h(5, dst, s->p.npx * sizeof(double), from, s->pitch * sizeof(double), s->p.npx * sizeof(double),
                        s->p.npy, s->st));
@@ -655,7 +820,7 @@ extern "C" int tsu_get_extrema(TsuSolver *s, double *hmax, double *bmin, double 
             d = s->stage64 + f * s->plane;
         }
         dst[n] = want[f];
-        from[n++] = d;
+        from[n++] = d + s->own_off();
     }
     CK(tsu::planes_d2h(n, dst, s->p.npx * sizeof(double), from, s->pitch * sizeof(double), s->p.npx * sizeof(double),
                        s->p.npy, s->st));
@@ -711,7 +876,7 @@ extern "C" int tsu_state_device(TsuSolver *s, void **ptr, long *pitch_elems, lon
     if (!s) return TSU_ERR_INVALID;
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->st));
-    if (ptr) *ptr = s->current();
+    if (ptr) *ptr = static_cast<char *>(s->current()) + s->own_off() * (long long)s->elem();
     if (pitch_elems) *pitch_elems = (long)s->pitch;
     if (plane_elems) *plane_elems = (long)s->plane;
     if (elem_bytes) *elem_bytes = (int)s->elem();

@@ -13,8 +13,16 @@ struct TsuSolver {
     TsuSwitches sw{};
     int device = 0;
     bool fp32 = false;
-    cudaStream_t st = nullptr;
-    long long pitch = 0, plane = 0;  // elements
+    cudaStream_t st = nullptr;     // the stream all work is issued on
+    cudaStream_t own_st = nullptr;  // the solver's own stream (st unless tsu_set_stream chose another)
+    long long pitch = 0, plane = 0;  // elements; a plane holds the stored rows
+    // Row slab of a decomposed grid (tsu_slab_create): p describes the owned
+    // rows only (p.npy of them, global rows j0 .. j0 + p.npy - 1 of a grid of
+    // ny_glob rows); gs / gn ghost rows are stored below / above them.  A
+    // whole grid has slab = false, j0 = gs = gn = 0, ny_glob = p.npy.
+    bool slab = false;
+    int j0 = 0, gs = 0, gn = 0, ny_glob = 0;
+    long long own_off() const { return (long long)gs * pitch; }  // elements to owned row 0
     // FP64 plain form: planes h, qx, qy, H, hc.  FP32 form: z, H, qx, qy, hc.
     void *A = nullptr, *B = nullptr;
     void *K = nullptr;  // MUSCL-Hancock (rk == 0) only: the unfiltered working state Vk
@@ -36,6 +44,7 @@ struct TsuSolver {
     cudaGraphExec_t graph_exec = nullptr;
     long last_launches = 0;
     bool has_state = false, ready = false, timed = false;
+    int fault = 0;  // status a kernel reported (TSU_ERR_CUDA / TSU_ERR_NONFINITE) until the next tsu_reset
     // TMA descriptors of A and B (interior tiles stage their loads by TMA)
     CUtensorMap tmA{}, tmB{};
     CUtensorMap tmM{};  // the mask (uint8 [npy][pitch])

@@ -189,9 +189,11 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
         Vout = par ? A.bufA : A.bufB;
     }
 
-    // tile and halo inside the grid, not periodic: no clamping, and every
-    // edge of the tile is an interior edge
-    const bool inner = !periodic && x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= npx && y0 + TY + 2 <= npy;
+    // tile and halo inside the stored rows (the owned rows and a slab's ghost
+    // rows), not periodic: no clamping, and every edge of the tile is an
+    // interior edge
+    const bool inner =
+        !periodic && x0 >= 2 && y0 - 2 >= -P.gs && x0 + TX + 2 <= npx && y0 + TY + 2 <= npy + P.gn;
 
     // ---- phase 1: tile + halo -> smem.  Interior tiles: one TMA box of the
     // 5 state planes (x0 - 2 doubles = a multiple of 16 bytes) and one of the
@@ -203,8 +205,9 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             mbar_init(&sBar, 1);
             mbar_init_fence();
             mbar_expect_tx(&sBar, 5 * PS * sizeof(double) + T::MPS);
-            tma_load_3d(sV, (Vin == A.bufB) ? &A.tmB : &A.tmA, x0 - 2, y0 - 2, 0, &sBar);
-            tma_load_2d(sM, &A.tmM, x0 - MHX, y0 - 2, &sBar);
+            // the tensor maps start at the first stored row (a slab's lowest ghost row)
+            tma_load_3d(sV, (Vin == A.bufB) ? &A.tmB : &A.tmA, x0 - 2, y0 - 2 + P.gs, 0, &sBar);
+            tma_load_2d(sM, &A.tmM, x0 - MHX, y0 - 2 + P.gs, &sBar);
         }
     } else {
         for (int idx = tid; idx < PS; idx += NT) {
@@ -212,7 +215,9 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             int gx = x0 + lx - 2, gy = y0 + ly - 2;
             if (!inner) {
                 gx = wrap_clamp(gx, npx, periodic);
-                gy = wrap_clamp(gy, npy, periodic);
+                // rows outside the stored ones: the grid's own boundary (a
+                // slab stores ghost rows wherever it has a neighbour)
+                if (gy < -P.gs || gy >= npy + P.gn) gy = wrap_clamp(gy, npy, periodic);
             }
             const long long g = (long long)gy * pitch + gx;
 #pragma unroll
@@ -393,12 +398,13 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             const double *Lf = sFx + r * FXW + (e + 1);
             nx = 1;
             ny = 0;
+            const int J = P.j0 + ey;  // the global row (boundary-series segments)
             if (periodic && (ex == 0 || ex == npx)) {  // seam: GPU/VolumeSolver.cu:262-275,289-298
                 a = get5(Rf, TY * FXW);
                 b = get5(Lf, TY * FXW);
                 fixed = sM[ly * MLX + e + 1 + (MHX - 2)];
                 seam = true;
-                seg = npx + ey;
+                seg = npx + J;
                 if (e >= 1) outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
                 if (e < TX) outP = sFlux + 0 * 5 * FS + r * TX + e;
             } else if (ex == 0) {  // west: GPU/VolumeSolver.cu:233-258
@@ -406,13 +412,13 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
                 nx = -1;
                 fixed = sM[ly * MLX + e + 2 + (MHX - 2)];
                 bnd = true;
-                seg = 2 * npx + npy + ey;
+                seg = 2 * npx + P.ny_glob + J;
                 outM = sFlux + 0 * 5 * FS + r * TX + e;
             } else if (ex == npx) {  // east: GPU/VolumeSolver.cu:276-298
                 a = get5(Rf, TY * FXW);
                 fixed = sM[ly * MLX + e + 1 + (MHX - 2)];
                 bnd = true;
-                seg = npx + ey;
+                seg = npx + J;
                 outM = sFlux + 1 * 5 * FS + r * TX + (e - 1);
             } else {  // interior: GPU/VolumeSolver.cu:300-314
                 a = get5(Rf, TY * FXW);
@@ -432,26 +438,30 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             const double *Df = sFy + (e + 1) * TX + c;
             nx = 0;
             ny = 1;
-            if (periodic && (ey == 0 || ey == npy)) {  // seam: GPU/VolumeSolver.cu:352-367,378-387
+            // the grid's own south / north boundary (a slab's other edges are
+            // interior edges, their far side in the ghost rows)
+            const int J = P.j0 + ey;
+            const bool south = (J == 0), north = (J == P.ny_glob);
+            if (periodic && (south || north)) {  // seam: GPU/VolumeSolver.cu:352-367,378-387
                 a = get5(Uf, FYH * TX);
                 b = get5(Df, FYH * TX);
                 fixed = sM[(e + 1) * MLX + c + 2 + (MHX - 2)];
                 seam = true;
-                seg = npx + npy + ex;
+                seg = npx + P.ny_glob + ex;
                 if (e >= 1) outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
                 if (e < TY) outP = sFlux + 2 * 5 * FS + e * TX + c;
-            } else if (ey == 0) {  // south: GPU/VolumeSolver.cu:324-349
+            } else if (south) {  // south: GPU/VolumeSolver.cu:324-349
                 a = get5(Df, FYH * TX);
                 ny = -1;
                 fixed = sM[(e + 2) * MLX + c + 2 + (MHX - 2)];
                 bnd = true;
                 seg = ex;
                 outM = sFlux + 2 * 5 * FS + e * TX + c;
-            } else if (ey == npy) {  // north: GPU/VolumeSolver.cu:352-387
+            } else if (north) {  // north: GPU/VolumeSolver.cu:352-387
                 a = get5(Uf, FYH * TX);
                 fixed = sM[(e + 1) * MLX + c + 2 + (MHX - 2)];
                 bnd = true;
-                seg = npx + npy + ex;
+                seg = npx + P.ny_glob + ex;
                 outM = sFlux + 3 * 5 * FS + (e - 1) * TX + c;
             } else {  // interior: GPU/VolumeSolver.cu:389-403
                 a = get5(Uf, FYH * TX);
@@ -469,7 +479,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             }
         }
         if ((bnd || seam) && P.read_files) {  // CC series while active, then wall
-            if (series_on) series_state(A.CC, A.tCC, t, npx, npy, seg, b);
+            if (series_on) series_state(A.CC, A.tCC, t, npx, P.ny_glob, seg, b);
             else if (vert) b.qx = -a.qx;
             else b.qy = -a.qy;
         }
@@ -608,7 +618,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             if (tid == 0) {
                 for (int w = 0; w < T::kRed; w++) mm = fmin(mm, sRed[w]);
                 A.scal[SC_T] = t + dt;
-                A.scal[SC_DT] = finalize_dt(mm, (long long)npx * npy);
+                A.scal[SC_DT] = finalize_dt(mm, (long long)npx * P.ny_glob);
                 A.scal[SC_STEPS] += 1.0;
                 if (PINGPONG) A.scal[SC_PAR] = (double)(1 - par);
                 *A.ticket = 0u;
@@ -659,7 +669,7 @@ __global__ void __launch_bounds__(256) dt_partials_kernel(const double *__restri
         __syncthreads();
         if (tid == 0) {
             for (int w = 0; w < 8; w++) mm = fmin(mm, sRed[w]);
-            scal[SC_DT] = finalize_dt(mm, (long long)P.npx * P.npy);
+            scal[SC_DT] = finalize_dt(mm, (long long)P.npx * P.ny_glob);
             *ticket = 0u;
             __threadfence();
         }
