@@ -25,9 +25,13 @@ larger than the 126 MB L2, so no L2 flush is needed between steps.
                   the oracle port on the host cores.  It never loads the
                   product library.
 
-Multi-GPU (torchrun, one rank per GPU): every rank advances its own replica
-(weak scaling, no data-path collective); the reported time is the max over
-ranks of the device-timed region.
+Multi-GPU (torchrun, one rank per GPU): the grid is split into row slabs,
+one per rank (tsuner_b200/slabs.py: a 2-row halo exchange per RK stage by
+NCCL send/recv, a MIN all-reduce of the dt per step; strong scaling of the
+one grid); --replicas runs one copy of the grid per rank instead (weak
+scaling, no data-path collective).  The ensemble workload shares its members
+out over the ranks.  The reported time is the max over ranks of the
+device-timed region.
 """
 import argparse
 import ctypes as C
@@ -340,13 +344,85 @@ def run_config3(a, T, local):
     return out
 
 
+def shard_members(ws, world, rank):
+    """Members of this rank: the largest first, each to the least loaded rank
+    (cells), so that the ranks' shares of the cell count stay close."""
+    load = [0] * world
+    mine = []
+    for i in sorted(range(len(ws)), key=lambda i: -ws[i].ncells):
+        r = min(range(world), key=lambda q: load[q])
+        load[r] += ws[i].ncells
+        if r == rank:
+            mine.append(ws[i])
+    return mine
+
+
+def run_decomposed(a, rank, world, local, dist):
+    """One grid split into row slabs, one per rank (tsuner_b200/slabs.py):
+    per RK stage a 2-row halo exchange by NCCL send/recv, per step a MIN
+    all-reduce of the dt; strong scaling of the single grid.  FP64 plain form
+    (the reference's arithmetic).  Device time: CUDA events on the stream the
+    slabs and their messages use, max over ranks."""
+    import torch
+
+    from tsuner_b200 import slabs as S
+    w, desc = workload(a.workload)
+    n = w.ncells
+    sw = form_switches(w, 0)
+    g = S.SlabGroup(w.p, sw, dist=dist, device=local)
+    g.load(w.V, w.mask, w.CC, w.tCC)
+    g.reset()
+    g.step(a.warmup)
+    g.sync()
+    barrier(dist, local)
+    st = torch.cuda.current_stream(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        e0.record(st)
+        g.step(a.steps)
+        e1.record(st)
+        g.sync()
+    ms = dist_max(dist, e0.elapsed_time(e1), local)
+    barrier(dist, local)
+    t0 = time.perf_counter()
+    g.load(w.V, w.mask, w.CC, w.tCC)
+    g.reset()
+    g.step(a.steps)
+    parts = g.local_state()
+    g.local_extrema()
+    e2e_s = dist_max(dist, time.perf_counter() - t0, local)
+    g.close()
+    assert all(np.isfinite(v).all() for _, v in parts.values())
+    if rank != 0:
+        return None
+    cfg = arm_config(desc, n, world)
+    cfg["parallelism"] = ("row slabs x%d (2-row halo of the 5 state planes per RK stage by NCCL send/recv into "
+                          "local buffers, 8-byte MIN all-reduce of dt per step)" % world)
+    return {
+        "metric": METRIC, "value": round(n * a.steps / (ms / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
+        "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4),
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generators, no dataset)", "config": cfg, "form": FORM[0],
+        "roofline": roofline("f64", n, a.steps, ms, "stage64_" + a.workload),
+        "gpu_launches": 2 * a.steps,
+        "e2e": {"value": round(n * a.steps / e2e_s / 1e6, 3), "unit": "Mcell-steps/s",
+                "h2d_bytes_per_step": int((5 * 8 * n + 4 * n + w.CC.nbytes + w.tCC.nbytes) / a.steps),
+                "d2h_bytes_per_step": int((5 * 8 * n + 3 * 8 * n) / a.steps),
+                "what": "every rank: its slab's upload, reset, K steps with the exchanges, read-back; max over ranks"},
+        "clocks": clk.summary(),
+    }
+
+
 def run_ensemble(a, rank, world, local, dist):
-    """Config 4: batched FP32 ensemble; value = sum(cells) x steps / time."""
+    """Config 4: batched FP32 ensemble; value = sum(cells) x steps / time.
+    With several GPUs the members are shared out among the ranks (no
+    exchange between members); the time is the max over ranks."""
     import tsuner_b200 as T
     from tsuner_b200 import workloads as W
     nmem = int(a.workload[len("ensemble"):] or 256)
-    ws = W.ensemble(nmembers=nmem)
-    cells = sum(w.ncells for w in ws)
+    ws_all = W.ensemble(nmembers=nmem)
+    ws = shard_members(ws_all, world, rank) if world > 1 else ws_all
+    cells = sum(w.ncells for w in ws_all)
     e = T.Ensemble([w.p for w in ws], [w.sw for w in ws], device=local)
     e.load(ws)
     e.reset()
@@ -382,27 +458,29 @@ def run_ensemble(a, rank, world, local, dist):
         return None
     hbm, kind = peaks()
     bpc = BYTES_PER_CELL_STEP["f32"]
-    achieved = bpc * cells * a.steps / (ms / 1e3) / 1e9
+    cells_here = sum(w.ncells for w in ws)  # this rank's share (rank 0)
+    achieved = bpc * cells_here * a.steps / (ms / 1e3) / 1e9
     h2d = sum(5 * 8 * w.ncells + 4 * w.ncells + w.CC.nbytes + w.tCC.nbytes for w in ws)
     d2h = sum(5 * 8 * w.ncells for w in ws)
     return {
-        "metric": METRIC, "value": round(world * cells * a.steps / (ms_max / 1e3) / 1e6, 3),
+        "metric": METRIC, "value": round(cells * a.steps / (ms_max / 1e3) / 1e6, 3),
         "unit": "Mcell-steps/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-        "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, no dataset)",
         "config": {"workload": "ensemble of %d members, square sides log-uniform in [256, 2048] (seed 4), "
                                "own shelf bathymetry / mask / west N-wave each" % nmem,
                    "cells": cells, "form": "fp32 precision form, one persistent launch per RK stage over all "
                                             "members, per-member dt, CUDA graph",
                    "tile": cfg, "autotune": report.strip().splitlines(),
-                   "parallelism": "replicas x%d" % world},
+                   "parallelism": ("members shared out over %d ranks (largest first to the least loaded; "
+                                   "no exchange)" % world) if world > 1 else "single GPU"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                      "frac": round(achieved / hbm, 4), "peak_kind": kind, "bytes_per_cell_step": bpc,
                      "traffic": None},
-        "members_one_by_one": {"value": round(cells * a.steps / (ms_seq / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
+        "members_one_by_one": {"value": round(cells_here * a.steps / (ms_seq / 1e3) / 1e6, 3), "unit": "Mcell-steps/s",
                                "ms_per_step": round(ms_seq / a.steps, 4)},
         "gpu_launches": launches,
-        "e2e": {"value": round(world * cells * a.steps / e2e_s / 1e6, 3), "unit": "Mcell-steps/s",
+        "e2e": {"value": round(cells * a.steps / e2e_s / 1e6, 3), "unit": "Mcell-steps/s",
                 "h2d_bytes_per_step": int(h2d / a.steps), "d2h_bytes_per_step": int(d2h / a.steps),
                 "what": "upload all members + reset + K steps + read all members back, host buffers"},
         "clocks": clk.summary(),
@@ -487,6 +565,8 @@ def run_ours(a, rank, world, local, dist):
         return run_ensemble(a, rank, world, local, dist)
     if a.workload == "corrector":
         return run_corrector(a, rank, world, local, dist)
+    if world > 1 and not a.replicas:
+        return run_decomposed(a, rank, world, local, dist)
     w, desc = workload(a.workload)
     n = w.ncells
     prim = 1 if a.precision == "fp32" else 0
@@ -603,6 +683,8 @@ def main():
     ap.add_argument("--no-other", "--no-fp64", dest="no_other", action="store_true",
                     help="skip the other form's run")
     ap.add_argument("--no-config3", action="store_true", help="skip the 8192^2 configuration")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with several GPUs: one copy of the grid per rank instead of one grid in row slabs")
     ap.add_argument("--config3-steps", type=int, default=2000, help="steps of the 8192^2 configuration")
     ap.add_argument("--corr-fine", type=int, default=512, help="corrector: fine grid side")
     ap.add_argument("--corr-train", type=int, default=128, help="corrector: training pairs")

@@ -192,7 +192,8 @@ int tsu_run_until(TsuSolver *s, double t_end, long max_steps, long *steps_done);
  * infinite (checked on the last RK stage of every step and by tsu_reset on
  * the uploaded state; the reference has no such check and steps on).  After
  * either, the solver steps again only after tsu_reset (and, for a
- * non-finite state, a new tsu_set_state).  tsu_get_time and tsu_run_until
+ * non-finite state, a new tsu_set_state); until then tsu_step / tsu_run_until
+ * return the same code without stepping.  tsu_get_time and tsu_run_until
  * report the same words; TSUNER() returns the code. */
 int tsu_sync(TsuSolver *s);
 /* 5*nvol doubles SoA (h, qx, qy, H, hc). */
@@ -362,6 +363,64 @@ int tsu_set_wait_limit_ns(unsigned long long ns);
  * their text in tsu_last_error(). */
 int tsu_cfl_dt_noalloc(const double *d_h, const double *d_qx, const double *d_qy, long pitch_elems,
                        const SimParams *p, double *d_dt, void *stream);
+/* ---------------- input pipeline (host only) ----------------
+ * The arithmetic of the reference's Read_files == 1 loader on grids the
+ * caller has already read (the reference reads them from NetCDF4 files,
+ * which needs libnetcdf / HDF5): each call restates one reference function,
+ * value for value.  Grids are row-major [ny][nx]; geographic coordinates in
+ * degrees, NCTR free surface and velocities in centimetres (the reference's
+ * UNITS = 0.01).  No device is touched. */
+/* interpolate_spherics (interpolations.cxx:779-865): the grid fun
+ * [npy_f][npx_f] with first cell centre (xmin_f + dx_f/2, ymin_f + dy_f/2)
+ * onto the npx x npy cell centres of [xmin, xmax] x [ymin, ymax] -> sol */
+int tsu_nctr_interp_grid(double xmin, double xmax, double ymin, double ymax, double xmin_f, double ymin_f,
+                         int npx_f, int npy_f, double dx_f, double dy_f, int npx, int npy, const double *fun,
+                         double *sol);
+/* fix_eta (interpolations.cxx:867-876), in place */
+int tsu_nctr_fix_eta(double *eta, const double *H, int npx, int npy, double slr);
+/* interpolate_CC (interpolations.cxx:368-775): boundary series CC
+ * [ntime][2npx + 2npy][4] from the NCTR grids ha / ua / va
+ * [ntime][nyg][nxg] (grid origin xmin_g, ymin_g, spacing dx_g, dy_g), the
+ * simulation box and its bed depth H [npy][npx] */
+int tsu_nctr_boundary_series(const double *ha, const double *ua, const double *va, unsigned long ntime, int nxg,
+                             int nyg, double xmin_g, double ymin_g, double dx_g, double dy_g, int npx, int npy,
+                             double xmin, double xmax, double ymin, double ymax, const double *H, double slr,
+                             double *CC);
+/* dy_transform + dx_transform (interpolations.cxx:79-94): metres per degree
+ * of latitude, per-row east-west spacing dxE[npy], the widest row's width */
+int tsu_nctr_sphere_metrics(double ymin, double dy, int npy, double xmax, double xmin, double dx, double *dxE,
+                            double *dy_unit, double *dmax);
+/* spheric2cartesian (interpolations.cxx:879-968) and spheric2cartesian_CC
+ * (:970-1097, in place) */
+int tsu_nctr_to_cartesian(double xmin, double xmax, double ymin, double ymax, const double *dxE, double dyE, int npx,
+                          int npy, const double *fun, double *sol);
+int tsu_nctr_to_cartesian_series(double xmin, double xmax, double ymin, double ymax, const double *dxE, double dyE,
+                                 int npx, int npy, unsigned long ntime, double *CC);
+/* value assignment (Problem_loader.cxx:576-605): H, h = eta * UNITS + H +
+ * slr (clipped at 0), zero discharge, mask = fix >= 0.5 (all 1 without a
+ * fix grid) */
+int tsu_nctr_assign_state(const double *H_cart, const double *eta_cart, const double *fix_cart, int npx, int npy,
+                          double slr, double *h, tsu_double2 *hu, double *H, int *fixH);
+/* The whole loader (Problem_loader.cxx:355-625, no sponge layer): bathymetry
+ * grid (lon xb[nxb], lat yb[nyb], bathy [nyb][nxb]), optional non-erodible
+ * grid (fix NULL: everything erodible), NCTR grids (lon xc, lat yc, times
+ * tgrid[ntime], ha / ua / va [ntime][nyc][nxc]) onto an npx x npy grid with
+ * sea-level rise slr.  Writes the box and spacing into p (xmin..ymax, dx,
+ * dy, npx, npy, nvol), the initial state h, (qx, qy), H, the mask, CC
+ * [ntime][2npx+2npy][4] and tCC [ntime]: the inputs of TSUNER(). */
+int tsu_nctr_prepare(int nxb, int nyb, const double *xb, const double *yb, const double *bathy, int nxf, int nyf,
+                     const double *xf, const double *yf, const double *fix, int nxc, int nyc, const double *xc,
+                     const double *yc, unsigned long ntime, const double *tgrid, const double *ha, const double *ua,
+                     const double *va, int npx, int npy, double slr, SimParams *p, double *h, tsu_double2 *hu,
+                     double *H, int *fixH, double *CC, double *tCC);
+/* tides_prep (tides.cxx:170-291): the tide grid [npt][nyt][nxt] (first
+ * longitude xp[0]) along the four boundaries -> tides_bd [npt][2npx+2npy];
+ * magnitudes above 1e5 become 0.  The reference computes it but its use on
+ * the device is commented out (GPU/VolumeSolver.cu:204-214), so TSUNER()
+ * accepts and ignores it, as the reference does. */
+int tsu_nctr_tides(const double *tides, int nxt, int nyt, unsigned long npt, const double *xp, int npx, int npy,
+                   double xmin, double xmax, double ymin, double ymax, double *tides_bd);
+
 /* Bulk host <-> device copies through the library's pinned staging chunks
  * and host worker pool, the path every tsu_set_* / tsu_get_* call of this
  * library uses (the reference copies with plain pageable cudaMemcpy,

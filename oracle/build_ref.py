@@ -113,18 +113,49 @@ def build_variant(name, ref=DEFAULT_REF, force=False):
     return so
 
 
+def build_interp(ref=DEFAULT_REF, force=False):
+    """oracle/_ref/interp/libref_interp.so: the reference's host input
+    interpolation (interpolations.cxx, tides.cxx, unmodified, g++ -O2 as the
+    reference makefile builds its host code) with ref_build/ref_interp_shim.cpp
+    and the in-memory netCDF stand-in ref_build/fake_netcdf.c."""
+    vdir = os.path.join(OUT, "interp")
+    os.makedirs(vdir, exist_ok=True)
+    so = os.path.join(vdir, "libref_interp.so")
+    rb = os.path.join(HERE, "ref_build")
+    srcs = [os.path.join(ref, "interpolations.cxx"), os.path.join(ref, "tides.cxx"),
+            os.path.join(rb, "ref_interp_shim.cpp")]
+    fake = os.path.join(rb, "fake_netcdf.c")
+    deps = srcs + [fake, os.path.join(rb, "netcdf.h"), __file__, os.path.join(ref, "TSUNER.h"),
+                   os.path.join(ref, "Sim_parameters.hxx")]
+    if not force and _newer(so, deps):
+        return so
+    inc = ["-I" + ref, "-I" + rb, "-I/usr/local/cuda/include"]
+    objs = []
+    for s in srcs:
+        o = os.path.join(vdir, os.path.basename(s) + ".o")
+        _run(["g++", "-O2", "-fPIC", "-w"] + inc + ["-c", s, "-o", o])
+        objs.append(o)
+    o = os.path.join(vdir, "fake_netcdf.o")
+    _run(["gcc", "-O2", "-fPIC", "-I" + rb, "-c", fake, "-o", o])
+    objs.append(o)
+    _run(["g++", "-shared", "-o", so] + objs)
+    for o in objs:
+        os.remove(o)
+    return so
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=DEFAULT_REF)
     ap.add_argument("--force", action="store_true")
-    ap.add_argument("variants", nargs="*")
+    ap.add_argument("variants", nargs="*", help="kernel variants (and/or 'interp'); default: all")
     a = ap.parse_args(argv)
     if not os.path.isdir(a.ref):
         print("reference tree not present; keeping prebuilt oracle/_ref")
         return 0
-    names = a.variants or [v + sfx for v in VARIANTS for sfx in ("", "-nolto")]
+    names = a.variants or [v + sfx for v in VARIANTS for sfx in ("", "-nolto")] + ["interp"]
     for v in names:
-        print(build_variant(v, a.ref, a.force))
+        print(build_interp(a.ref, a.force) if v == "interp" else build_variant(v, a.ref, a.force))
     return 0
 
 

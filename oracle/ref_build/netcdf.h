@@ -55,6 +55,7 @@ int nc_get_vara_double(int ncid, int varid, const size_t *startp, const size_t *
 int nc_get_var_float(int ncid, int varid, float *ip);
 int nc_get_vara_float(int ncid, int varid, const size_t *startp, const size_t *countp, float *ip);
 int nc_inq_var(int ncid, int varid, char *name, nc_type *xtypep, int *ndimsp, int *dimidsp, int *nattsp);
+int nc_get_att_int(int ncid, int varid, const char *name, int *ip);
 
 #ifdef __cplusplus
 }

@@ -71,7 +71,7 @@ def test_expired_tile_wait_is_reported_and_the_solver_recovers(precision, short_
     rc = T.lib().tsu_sync(s._h)
     assert rc == TSU_ERR_CUDA, rc
     assert b"expired" in T.lib().tsu_last_error()
-    assert T.lib().tsu_step(s._h, 1) != 0  # refuses to step until reset
+    assert T.lib().tsu_step(s._h, 1) == TSU_ERR_CUDA  # refuses to step until reset
     short_waits(0)
     s.set_state(w.V)
     s.reset()
@@ -184,13 +184,14 @@ def test_nan_appearing_between_steps_is_reported(precision):
         off = (f * plane + 25 * pitch + 35) * eb
         bad = np.array([np.nan], np.float64 if eb == 8 else np.float32)
         assert T.lib().tsu_copy_bytes_to_device(0, C.c_void_p(ptr + off), bad.ctypes.data_as(C.c_void_p), eb) == 0
-        s.step(1)
-        with pytest.raises(T.TsunerError) as ei:
-            s.sync()
-        assert ei.value.code == TSU_ERR_NONFINITE
-        with pytest.raises(T.TsunerError) as ei:
+        with pytest.raises(T.TsunerError) as ei:  # run_until checks after each chunk of steps
             s.run_until(1e9, 4)
         assert ei.value.code == TSU_ERR_NONFINITE
+        with pytest.raises(T.TsunerError) as ei:  # the device's status word stays set
+            s.sync()
+        assert ei.value.code == TSU_ERR_NONFINITE
+        assert T.lib().tsu_step(s._h, 1) == TSU_ERR_NONFINITE  # no stepping until reset
+        assert b"tsu_reset" in T.lib().tsu_last_error()
     finally:
         s.close()
 

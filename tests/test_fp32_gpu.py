@@ -20,9 +20,13 @@ from tsuner_b200.abi import make_switches
 
 pytestmark = pytest.mark.gpu
 
-# L-inf depth difference to the FP64 form after 400 steps.  It is set by the
+# L-inf depth difference to the FP64 form after 400 steps on these small,
+# coarse grids (10 m cells, fronts a few cells wide).  It is set by the
 # wet/dry front cells, where FP32 and FP64 runs may wet a cell one step apart;
 # away from fronts the difference is ~1e-6 m (see the L2 in bench.py).
+# Measured on a B200: 3.1e-4 m (shelf) and 1.26e-3 m (run-up).  The 1e-4 m
+# bar of the FP32 form is asserted on the 8192^2 configuration it is stated
+# for (test_config3_humps8192_2000_steps_within_1e4_m, measured 7.5e-5 m).
 DEPTH_LINF_M = 5e-4     # coarse shelf, 3 m N-wave reaching the beach
 RUNUP_LINF_M = 2e-3     # Gaussian hump running up a beach (strong wet/dry fronts)
 MASS_REL = 1e-6

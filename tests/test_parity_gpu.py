@@ -257,10 +257,18 @@ def test_switch_variants_vs_reference_build(variant, sw):
 def test_manning_vs_reference_build():
     """The reference's unfinished Manning branch (GPU/Reconstructor.cu:47-50,
     momentum multiplied by c) on an all-wet hump: a dry cell gives 0/0 there,
-    which this build reports as a non-finite state."""
+    which this build reports as a non-finite state.  Value for value against
+    the -nolto build of the reference sources.  The recipe (-dlto) build
+    rounds the per-cell pow() of this branch differently in the last bit and
+    the branch rescales the momentum by it every step, so the recipe build
+    drifts from its own -nolto twin by ~3e-11 relative in h after 100 steps
+    (measured on a B200); it is held to 1e-10 here."""
     w = W.hump(72, 56, 10.0, sigma=120.0)
     assert (w.V[0] > 0).all()
-    ref_vs_new(w, 100, "manning_rf0", make_switches(order=2, wbc=1, read_files=0, manning=1))
+    new, ref = ref_vs_new(w, 100, "manning_rf0", make_switches(order=2, wbc=1, read_files=0, manning=1),
+                          recipe_tol=1e-10)
+    print("manning: recipe build vs the product: " +
+          ", ".join("%s %.2e" % (name, rel_err(new["V"][f], ref["V"][f])) for f, name in enumerate(FIELDS)))
 
 
 @need_ref

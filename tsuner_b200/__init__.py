@@ -40,6 +40,9 @@ EXPORTS = [
     "tsu_corr_last_error", "tsu_set_wait_limit_ns",
     "tsu_slab_create", "tsu_slab_info", "tsu_slab_halo_bytes", "tsu_slab_pack", "tsu_slab_unpack", "tsu_slab_stage",
     "tsu_get_dt_device", "tsu_set_dt_device", "tsu_set_stream",
+    "tsu_nctr_interp_grid", "tsu_nctr_fix_eta", "tsu_nctr_boundary_series", "tsu_nctr_sphere_metrics",
+    "tsu_nctr_to_cartesian", "tsu_nctr_to_cartesian_series", "tsu_nctr_assign_state", "tsu_nctr_prepare",
+    "tsu_nctr_tides",
 ]
 
 _ENS_SIG = {
@@ -142,6 +145,22 @@ def lib():
             "tsu_get_dt_device": ([vp, vp], C.c_int),
             "tsu_set_dt_device": ([vp, vp], C.c_int),
             "tsu_set_stream": ([vp, vp], C.c_int),
+            "tsu_nctr_interp_grid": ([C.c_double] * 6 + [C.c_int] * 2 + [C.c_double] * 2 + [C.c_int] * 2 + [vp, vp],
+                                     C.c_int),
+            "tsu_nctr_fix_eta": ([vp, vp, C.c_int, C.c_int, C.c_double], C.c_int),
+            "tsu_nctr_boundary_series": ([vp, vp, vp, C.c_ulong, C.c_int, C.c_int] + [C.c_double] * 4 +
+                                         [C.c_int] * 2 + [C.c_double] * 4 + [vp, C.c_double, vp], C.c_int),
+            "tsu_nctr_sphere_metrics": ([C.c_double, C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
+                                         vp, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+            "tsu_nctr_to_cartesian": ([C.c_double] * 4 + [vp, C.c_double, C.c_int, C.c_int, vp, vp], C.c_int),
+            "tsu_nctr_to_cartesian_series": ([C.c_double] * 4 + [vp, C.c_double, C.c_int, C.c_int, C.c_ulong, vp],
+                                             C.c_int),
+            "tsu_nctr_assign_state": ([vp, vp, vp, C.c_int, C.c_int, C.c_double, vp, vp, vp, vp], C.c_int),
+            "tsu_nctr_prepare": ([C.c_int, C.c_int, vp, vp, vp, C.c_int, C.c_int, vp, vp, vp, C.c_int, C.c_int, vp,
+                                  vp, C.c_ulong, vp, vp, vp, vp, C.c_int, C.c_int, C.c_double,
+                                  C.POINTER(SimParams), vp, vp, vp, vp, vp, vp], C.c_int),
+            "tsu_nctr_tides": ([vp, C.c_int, C.c_int, C.c_ulong, vp, C.c_int, C.c_int] + [C.c_double] * 4 + [vp],
+                               C.c_int),
             "checkCUDAsupport": ([C.c_int], C.c_int),
             "initializeGPU": ([], None),
         }

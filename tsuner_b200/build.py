@@ -30,6 +30,9 @@ UNIT_FLAGS = {
     # FP32 precision form: single precision may contract and use the hardware
     # approximations; its FP64 islands are unaffected by this flag.
     "stage32.cu": ["-use_fast_math"],
+    # host restatement of the reference's input interpolation: no contraction,
+    # like the reference's host build
+    "nctr.cpp": ["-Xcompiler", "-ffp-contract=off"],
 }
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC]
 
@@ -67,7 +70,7 @@ def build(force=False, verbose=False):
         if force or _stale(obj, [src] + hdrs):
             cmd = [NVCC] + ARCH + COMMON + UNIT_FLAGS.get(f, []) + ["-c", src, "-o", obj]
             if f.endswith(".cpp"):
-                cmd = [NVCC] + COMMON + ["-x", "c++", "-c", src, "-o", obj]
+                cmd = [NVCC] + COMMON + UNIT_FLAGS.get(f, []) + ["-x", "c++", "-c", src, "-o", obj]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
             r = _run(cmd)

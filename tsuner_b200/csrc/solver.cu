@@ -73,11 +73,12 @@ int tsu_device_flags(TsuSolver *s, const double *sc) {
     return TSU_OK;
 }
 
-// a solver whose kernels reported an error steps again only after tsu_reset
+// a solver whose kernels reported an error steps again only after tsu_reset;
+// until then stepping calls return that error
 static int fault_refuses(TsuSolver *s, const char *what) {
     snprintf(g_err, sizeof(g_err), "%s: the last steps reported %s; tsu_reset (after tsu_set_state for a "
              "non-finite state) before stepping again", what, tsu_strerror(s->fault));
-    return TSU_ERR_INVALID;
+    return s->fault;
 }
 
 static int device_flags(TsuSolver *s) {
