@@ -509,6 +509,7 @@ def run_corrector(a, rank, world, local, dist):
     t_truth = time.perf_counter() - t0
     c = K.Corrector(n, n, f, max_batch=8, device=local)
     c.set_site(site.H)
+    c.set_options(a.corr_wbig, a.corr_clip)
     c.add_samples(coarse_train, fine_train)
     c.add_samples(coarse_test, truth)
     # step-wise decay: half the steps at 1e-3, a quarter at 3e-4, a quarter at 1e-4
@@ -526,8 +527,9 @@ def run_corrector(a, rank, world, local, dist):
     with Clocks(local) as clk:
         ms_conv, tflops = c.bench_conv(8, max(a.steps, 5))
     c.close()
-    e_with = K.errors((oh, ob), truth)
-    e_without = K.errors((bh, bb), truth)
+    region = (truth[:, 0] > 0) | (oh != 0) | (bh != 0)  # one denominator for both RMSEs
+    e_with = K.errors((oh, ob), truth, region)
+    e_without = K.errors((bh, bb), truth, region)
     if rank != 0:
         return None
     try:
@@ -545,6 +547,7 @@ def run_corrector(a, rank, world, local, dist):
                                % (n, n, site.dx, n // f, n // f, len(train_src), len(test_src), t_end),
                    "network": "6 x conv3x3 32 ch, BF16 weights/activations, FP32 accumulate (tcgen05, TMEM)",
                    "train": {"iters": a.corr_iters, "batch": 8, "lr": "1e-3 / 3e-4 / 1e-4 (1/2, 1/4, 1/4 of the steps)",
+                             "large_residual_weight": a.corr_wbig, "clip_depth": bool(a.corr_clip),
                              "ms": round(train_ms, 1),
                              "convs": convs, "loss_first": float(loss[:5].mean()),
                              "loss_last": float(loss[-10:].mean())},
@@ -691,6 +694,10 @@ def main():
     ap.add_argument("--corr-test", type=int, default=16, help="corrector: held-out sources")
     ap.add_argument("--corr-iters", type=int, default=400, help="corrector: Adam steps")
     ap.add_argument("--corr-tend", type=float, default=600.0, help="corrector: simulated seconds per source")
+    ap.add_argument("--corr-wbig", type=float, default=0.0,
+                    help="corrector: loss weight 1 + w t^2 on large maximum-depth residuals")
+    ap.add_argument("--corr-clip", type=int, default=0, choices=[0, 1],
+                    help="corrector: clip the corrected maximum depth at 0")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     a.config3_steps = max(a.config3_steps, 10)

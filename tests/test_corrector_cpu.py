@@ -45,3 +45,9 @@ def test_error_metric():
     assert np.isclose(e["hmax_rmse_m"], np.sqrt((0.25 + 0.0625) / wet))
     assert np.isclose(e["hmax_linf_m"], 0.5)
     assert np.isclose(e["db_rmse_m"], 0.1)
+    ph[0, 3, 0] = -0.5      # a negative maximum depth counts as an error
+    e = K.errors((ph, pb), truth)
+    assert np.isclose(e["hmax_rmse_m"], np.sqrt((0.25 + 0.0625 + 0.25) / 10))
+    region = truth[:, 0] > 0  # an explicit region sets the denominator
+    e = K.errors((ph, pb), truth, region)
+    assert np.isclose(e["hmax_rmse_m"], np.sqrt(0.25 / 8)) and np.isclose(e["hmax_linf_m"], 0.5)

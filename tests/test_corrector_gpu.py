@@ -168,6 +168,37 @@ def test_untrained_corrector_is_interpolation_and_training_lowers_loss():
         c.close()
 
 
+def test_options_weight_large_residuals_and_clip_depth():
+    dev()
+    ny, f = 64, 4
+    Hf, coarse, fine = synthetic_samples(8, ny, f, 7)
+    first = []
+    for wbig in (0.0, 4.0):
+        c = K.Corrector(ny, ny, f, max_batch=4, seed=3)
+        try:
+            c.set_site(Hf)
+            c.set_options(wbig, False)
+            c.add_samples(coarse, fine)
+            loss = c.train(ntrain=8, iters=40, batch=4, lr=2e-3, seed=1)
+            assert np.isfinite(loss).all() and loss[-5:].mean() < loss[:3].mean()
+            first.append(float(loss[0]))
+            oh, _, _, _ = c.predict(0, 8)
+            c.set_options(wbig, True)
+            ohc, _, _, _ = c.predict(0, 8)
+            assert (ohc >= 0).all()
+            assert np.array_equal(ohc, np.maximum(oh, 0.0))
+        finally:
+            c.close()
+    # same weights and batch at the first step: the weighted loss is larger
+    assert first[1] > first[0], first
+    c = K.Corrector(ny, ny, f, max_batch=4, seed=3)
+    try:
+        for bad in ((-1.0, 0), (0.0, 2)):
+            assert T.lib().tsu_corr_set_options(c._h, *bad) != 0
+    finally:
+        c.close()
+
+
 def test_set_weights_round_trip_and_conv_bench():
     dev()
     ny, f = 32, 4

@@ -30,12 +30,14 @@ EXPORTS = [
     "tsu_reset", "tsu_step", "tsu_run_until", "tsu_sync", "tsu_get_state", "tsu_get_extrema",
     "tsu_get_time", "tsu_get_sums", "tsu_get_consts", "tsu_last_step_ms", "tsu_last_step_launches",
     "tsu_state_device", "tsu_cfl_dt_noalloc", "tsu_copy_planes_to_device", "tsu_copy_planes_to_host",
-    "tsu_copy_bytes_to_device", "tsu_copy_bytes_to_host", "tsu_host_threads", "tsu_strerror", "tsu_last_error", "tsu_version", "tsu_struct_sizes",
+    "tsu_copy_bytes_to_device", "tsu_copy_bytes_to_host", "tsu_host_threads", "tsu_strerror", "tsu_last_error",
+    "tsu_version", "tsu_struct_sizes",
     "tsu_ens_create", "tsu_ens_destroy", "tsu_ens_member", "tsu_ens_reset", "tsu_ens_step", "tsu_ens_sync",
     "tsu_ens_autotune", "tsu_ens_set_config", "tsu_ens_get_config", "tsu_ens_last_step_ms",
     "tsu_ens_last_step_launches", "tsu_ens_run_until",
     "tsu_corr_create", "tsu_corr_destroy", "tsu_corr_set_site", "tsu_corr_add_samples", "tsu_corr_num_samples",
-    "tsu_corr_get_weights", "tsu_corr_set_weights", "tsu_corr_train", "tsu_corr_predict", "tsu_corr_bench_conv",
+    "tsu_corr_get_weights", "tsu_corr_set_weights", "tsu_corr_train", "tsu_corr_set_options", "tsu_corr_predict",
+    "tsu_corr_bench_conv",
     "tsu_corr_last_train_ms", "tsu_corr_conv3x3", "tsu_corr_conv3x3_wgrad", "tsu_corr_status",
     "tsu_corr_last_error", "tsu_set_wait_limit_ns",
     "tsu_slab_create", "tsu_slab_info", "tsu_slab_halo_bytes", "tsu_slab_pack", "tsu_slab_unpack", "tsu_slab_stage",
@@ -68,6 +70,7 @@ _ENS_SIG = {
     "tsu_corr_set_weights": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "tsu_corr_train": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_ulonglong, C.c_void_p], C.c_int),
     "tsu_corr_predict": ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 4, C.c_int),
+    "tsu_corr_set_options": ([C.c_void_p, C.c_float, C.c_int], C.c_int),
     "tsu_corr_bench_conv": ([C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "tsu_corr_last_train_ms": ([C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)], C.c_int),
     "tsu_corr_conv3x3": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,

@@ -87,6 +87,10 @@ class Corrector:
         _ck(lib().tsu_corr_train(self._h, ntrain, iters, batch, lr, seed, _fp(loss)), "tsu_corr_train")
         return loss[:iters]
 
+    def set_options(self, large_residual_weight=0.0, clip_depth=False):
+        _ck(lib().tsu_corr_set_options(self._h, float(large_residual_weight), int(bool(clip_depth))),
+            "tsu_corr_set_options")
+
     def predict(self, first, n):
         shp = (n, self.ny, self.nx)
         oh, ob, bh, bb = (np.empty(shp, np.float32) for _ in range(4))
@@ -199,12 +203,15 @@ def coarse_inputs(site, sources, t_end, chunk=128):
     return np.concatenate([maps, Hc], axis=1)
 
 
-def errors(pred, truth):
-    """RMSE and L-inf of maximum depth over cells wet in either map, and RMSE
-    of bed change, per sample averaged."""
+def errors(pred, truth, region=None):
+    """RMSE and L-inf of maximum depth over `region` (default: cells wet in
+    the truth or with a non-zero predicted maximum depth -- a negative one is
+    an error too), and RMSE of bed change over all cells.  Pass the same
+    region when comparing two predictions so that both RMSEs share one
+    denominator."""
     ph, pb = pred
     th, tb = truth[:, 0], truth[:, 1]
-    wet = (th > 0) | (ph > 0)
+    wet = ((th > 0) | (ph != 0)) if region is None else region
     dh = np.where(wet, ph - th, 0.0)
     rm = float(np.sqrt((dh ** 2).sum() / max(wet.sum(), 1)))
     linf = float(np.abs(dh).max())

@@ -615,19 +615,24 @@ __global__ void features_kernel(const int *__restrict__ idx, int nb, const float
     }
 }
 
-// Mean-square loss over the 2 output channels; dY = d(loss)/d(output) in
-// BF16 (channels 2..31 zero); loss sum accumulated in FP64.
-__global__ void loss_kernel(const float *__restrict__ Y, const float *__restrict__ T, long long npix,
+// Mean-square loss over the 2 output channels, each pixel's maximum-depth
+// term weighted by 1 + wbig * T^2 (T: the normalised residual target), so
+// that the few large residuals at run-up fronts weigh more than their share
+// of pixels; dY = d(loss)/d(output) in BF16 (channels 2..31 zero); loss sum
+// accumulated in FP64.
+__global__ void loss_kernel(const float *__restrict__ Y, const float *__restrict__ T, long long npix, float wbig,
                             bf16 *__restrict__ dY, double *__restrict__ loss) {
     __shared__ double sred[32];
-    const float scale = 1.f / (float)npix;  // d/dy of sum(d^2) / (2 npix)
+    const float scale = 1.f / (float)npix;  // d/dy of sum(w d^2) / (2 npix)
     double acc = 0.0;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
          p += (long long)gridDim.x * blockDim.x) {
-        const float d0 = Y[p * C] - T[p * 2], d1 = Y[p * C + 1] - T[p * 2 + 1];
-        acc += (double)d0 * d0 + (double)d1 * d1;
+        const float t0 = T[p * 2];
+        const float w0 = 1.f + wbig * t0 * t0;
+        const float d0 = Y[p * C] - t0, d1 = Y[p * C + 1] - T[p * 2 + 1];
+        acc += (double)w0 * d0 * d0 + (double)d1 * d1;
         uint4 *g = reinterpret_cast<uint4 *>(dY + p * C);
-        g[0] = make_uint4(pack2(scale * d0, scale * d1), 0, 0, 0);
+        g[0] = make_uint4(pack2(scale * w0 * d0, scale * d1), 0, 0, 0);
         g[1] = g[2] = g[3] = make_uint4(0, 0, 0, 0);
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -671,12 +676,14 @@ __global__ void adam_kernel(float *__restrict__ Wm, float *__restrict__ mW, floa
     }
 }
 
-// corrected fields: base + scale * output channel
+// corrected fields: base + scale * output channel; a maximum depth is not
+// negative (0 = never wet), so the corrected one is clipped at 0 when asked
 __global__ void apply_kernel(const float *__restrict__ Y, const float *__restrict__ base, long long npix,
-                             float *__restrict__ out_h, float *__restrict__ out_b) {
+                             int clip_depth, float *__restrict__ out_h, float *__restrict__ out_b) {
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
          p += (long long)gridDim.x * blockDim.x) {
-        out_h[p] = base[p * 2] + kSh * Y[p * C];
+        const float hc = base[p * 2] + kSh * Y[p * C];
+        out_h[p] = clip_depth ? fmaxf(hc, 0.f) : hc;
         out_b[p] = base[p * 2 + 1] + kSb * Y[p * C + 1];
     }
 }
@@ -797,6 +804,9 @@ struct TsuCorrector {
     int nsamples = 0, cap = 0;
     double last_ms = 0.0;
     long last_convs = 0;
+    // options (tsu_corr_set_options)
+    float wbig = 0.f;
+    int clip_depth = 0;
 };
 
 namespace {
@@ -1027,6 +1037,13 @@ extern "C" int tsu_corr_num_samples(TsuCorrector *c, int *n) {
     return TSU_OK;
 }
 
+extern "C" int tsu_corr_set_options(TsuCorrector *c, float large_residual_weight, int clip_depth) {
+    if (!c || !(large_residual_weight >= 0.f) || (clip_depth != 0 && clip_depth != 1)) return TSU_ERR_INVALID;
+    c->wbig = large_residual_weight;
+    c->clip_depth = clip_depth;
+    return TSU_OK;
+}
+
 extern "C" int tsu_corr_get_weights(TsuCorrector *c, float *W, float *B) {
     if (!c || !W || !B) return TSU_ERR_INVALID;
     CCK(cudaSetDevice(c->device));
@@ -1064,7 +1081,7 @@ extern "C" int tsu_corr_train(TsuCorrector *c, int ntrain, int iters, int batch,
         if (rc) break;
         e = cudaMemsetAsync(c->d_loss, 0, 8, c->st);
         if (e != cudaSuccess) break;
-        loss_kernel<<<4 * num_sms(), 256, 0, c->st>>>(c->Yout, c->T, npix, c->g0, c->d_loss);
+        loss_kernel<<<4 * num_sms(), 256, 0, c->st>>>(c->Yout, c->T, npix, c->wbig, c->g0, c->d_loss);
         if ((e = cudaGetLastError()) != cudaSuccess) break;
         if ((e = cudaMemcpyAsync(h_loss + it, c->d_loss, 8, cudaMemcpyDeviceToHost, c->st)) != cudaSuccess) break;
         if ((e = cudaMemsetAsync(c->gW, 0, nw * 4, c->st)) != cudaSuccess) break;
@@ -1131,7 +1148,8 @@ extern "C" int tsu_corr_predict(TsuCorrector *c, int first, int n, float *out_hm
         rc = load_batch(c, &s, 1, false);
         if (!rc) rc = forward(c, 1);
         if (rc) break;
-        apply_kernel<<<2 * num_sms(), 256, 0, c->st>>>(c->Yout, c->base, (long long)np, d_out, d_out + np);
+        apply_kernel<<<2 * num_sms(), 256, 0, c->st>>>(c->Yout, c->base, (long long)np, c->clip_depth, d_out,
+                                                         d_out + np);
         void *outs[2] = {out_hmax + k * np, out_db + k * np};
         const void *ins[2] = {d_out, d_out + np};
         if (cudaGetLastError() != cudaSuccess ||

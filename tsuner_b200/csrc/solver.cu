@@ -297,8 +297,9 @@ static int create_solver(TsuSolver **out, const SimParams *pg, const TsuSwitches
             s->tmM = t32.m;
         } else {
             // the maps cover every stored row (ghost rows included)
-            s->tma = stage64_tma_maps((const double *)s->A, (const double *)s->B, s->mask, s->pitch, s->plane, p->npx,
-                                      nstore, &s->tmA, &s->tmB, &s->tmM);
+            const double *ext[3] = {(const double *)s->hmax, (const double *)s->bmin, (const double *)s->eta};
+            s->tma = stage64_tma_maps((const double *)s->A, (const double *)s->B, s->mask, ext, s->pitch, s->plane,
+                                      p->npx, nstore, &s->tmA, &s->tmB, &s->tmM, &s->tmO, s->tmE);
         }
     }
     if (e != cudaSuccess) {
@@ -479,6 +480,8 @@ Stage64Args TsuSolver::args() const {
     a.tmA = tmA;
     a.tmB = tmB;
     a.tmM = tmM;
+    a.tmO = tmO;
+    for (int k = 0; k < 3; k++) a.tmE[k] = tmE[k];
     a.tma = tma ? 1 : 0;
     return a;
 }

@@ -48,6 +48,8 @@ struct TsuSolver {
     // TMA descriptors of A and B (interior tiles stage their loads by TMA)
     CUtensorMap tmA{}, tmB{};
     CUtensorMap tmM{};  // the mask (uint8 [npy][pitch])
+    CUtensorMap tmO{};  // FP64: the owned-cell boxes of A and of the extrema
+    CUtensorMap tmE[3]{};
     bool tma = false;
 
     tsu::Stage64Args args() const;

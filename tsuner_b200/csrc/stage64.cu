@@ -52,8 +52,14 @@ struct Tile {
     // tile (a 16-byte aligned TMA origin for bytes), 128-byte aligned
     static constexpr int MHX = 16, MLX = TX + 2 * MHX, MPS = MLX * LY;
     static constexpr size_t kMaskOff = (sizeof(double) * kDoubles + 127) / 128 * 128;
+    // the owned cells' U^n (5 planes) and running extrema (3 planes), [8][TY][TX],
+    // staged by TMA in the second RK stage (OWN == 2), 128-byte aligned
+    static constexpr size_t kOwnOff = (kMaskOff + MPS + 127) / 128 * 128;
+    static constexpr size_t kOwnBytes = 8 * TX * TY * sizeof(double);
     // + 128: the base is rounded up to 128 bytes (TMA destination)
-    static constexpr size_t smem() { return kMaskOff + MPS + 16 + 128; }
+    static constexpr size_t smem(bool staged_own = false) {
+        return (staged_own ? kOwnOff + kOwnBytes : kMaskOff + MPS + 16) + 128;
+    }
 };
 
 __device__ __forceinline__ int wrap_clamp(int g, int n, bool periodic) {
@@ -143,19 +149,25 @@ __device__ __forceinline__ void put5a(double *base, int stride, const double D[5
 // (FIRST = LAST = true), the state ping-pongs between bufA and bufB like the
 // order-1 form, and bufK holds the unfiltered working state Vk that the
 // reference carries from step to step (GPU/Volume_kernel.cu:283-299).
-// LATE: U^n of the owned cell (second RK stage) and its running extrema are
-// requested into L2 at tile start and loaded in the update, instead of U^n
-// being held in registers through the face and edge phases.
-template <int TX, int TY, int NTHR, int MINB, int ORDER, bool FIRST, bool LAST, bool RK0 = false, bool LATE = false>
+// OWN: where the second RK stage keeps U^n of the owned cell and its running
+// extrema between tile start and the update.  0: U^n loaded into registers
+// at tile start (held through the face and edge phases), extrema loaded in
+// the update; 1: both requested into L2 at tile start and loaded in the
+// update; 2: interior tiles stage both into shared memory with TMA boxes
+// issued at tile start (they land during the face and edge phases), other
+// tiles as 1.
+template <int TX, int TY, int NTHR, int MINB, int ORDER, bool FIRST, bool LAST, bool RK0 = false, int OWN = 0>
 __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_constant__ Stage64Args A) {
     static_assert(!RK0 || (FIRST && LAST), "MUSCL-Hancock is a single stage");
     constexpr bool PINGPONG = (ORDER == 1) || RK0;
+    constexpr bool LATE = (OWN >= 1);
     using T = Tile<TX, TY, NTHR>;
     constexpr int NT = T::NT, LX = T::LX, LY = T::LY, PS = T::PS, FXW = T::FXW, FYH = T::FYH;
     constexpr int MHX = T::MHX, MLX = T::MLX;
     extern __shared__ __align__(16) double smem_raw[];
     double *smem = smem_align<128>(smem_raw);
-    __shared__ uint64_t sBar;  // the tile's TMA load
+    __shared__ uint64_t sBar;     // the tile's TMA load
+    __shared__ uint64_t sBarOwn;  // OWN == 2: the owned cells' U^n and extrema
     const Phys64 &P = A.phys;
     double *sV = smem;                  // [5][LY][LX]
     double *sUC = smem + T::kSV;        // [3][LY][LX]  (ux, uy, c)
@@ -203,14 +215,28 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
     // mask (from x0 - 16); boundary tiles (clamped or wrapped halo) with
     // ordinary loads.
     const bool use_tma = inner && A.tma;
+    // the owned cells of an interior tile lie inside the stored rows: the
+    // boxes at (x0, y0) are in bounds, x0 * 8 bytes a multiple of 256
+    const bool own_tma = (OWN == 2) && !FIRST && use_tma;
+    constexpr int TC = TX * TY;
+    double *sOwn = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(smem) + T::kOwnOff);
     if (use_tma) {
         if (tid == 0) {
             mbar_init(&sBar, 1);
+            if (own_tma) mbar_init(&sBarOwn, 1);
             mbar_init_fence();
             mbar_expect_tx(&sBar, 5 * PS * sizeof(double) + T::MPS);
             // the tensor maps start at the first stored row (a slab's lowest ghost row)
             tma_load_3d(sV, (Vin == A.bufB) ? &A.tmB : &A.tmA, x0 - 2, y0 - 2 + P.gs, 0, &sBar);
             tma_load_2d(sM, &A.tmM, x0 - MHX, y0 - 2 + P.gs, &sBar);
+            if (own_tma) {
+                mbar_expect_tx(&sBarOwn, (LAST ? 8 : 5) * TC * sizeof(double));
+                tma_load_3d(sOwn, &A.tmO, x0, y0 + P.gs, 0, &sBarOwn);
+                if (LAST) {
+#pragma unroll
+                    for (int f = 0; f < 3; f++) tma_load_2d(sOwn + (5 + f) * TC, &A.tmE[f], x0, y0 + P.gs, &sBarOwn);
+                }
+            }
         }
     } else {
         for (int idx = tid; idx < PS; idx += NT) {
@@ -234,14 +260,14 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
     const bool own = cell_thread && (gi < npx) && (gj < npy);
     const long long gown = (long long)(own ? gj : 0) * pitch + (own ? gi : 0);
     double v0[5];
-    if (!FIRST) {  // U^n of the owned cell (friction, erosion, RK combine)
+    if (!FIRST && !own_tma) {  // U^n of the owned cell (friction, erosion, RK combine)
 #pragma unroll
         for (int f = 0; f < 5; f++) {
             if (LATE) prefetch_l2(V0 + f * plane + gown);
             else v0[f] = V0[f * plane + gown];
         }
     }
-    if (LATE && LAST && own) {
+    if (LATE && LAST && own && !own_tma) {
         prefetch_l2(A.hmax + gown);
         prefetch_l2(A.bmin + gown);
         prefetch_l2(A.eta_max + gown);
@@ -253,6 +279,7 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
             if (tid == 0) {
                 A.scal[SC_ERR] = 1.0;
                 mbar_wait(&sBar, 0);
+                if (own_tma) mbar_wait(&sBarOwn, 0);
             }
             return;
         }
@@ -501,13 +528,25 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
     }
     __syncthreads();
 
+    if (own_tma) {  // the owned cells' U^n and extrema have landed (bounded wait)
+        const bool ok = mbar_wait_first(&sBarOwn, 0);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                A.scal[SC_ERR] = 1.0;
+                mbar_wait(&sBarOwn, 0);
+            }
+            return;
+        }
+    }
+
     // ---- phase 5: cell update
     double dtcell = CUDART_INF;
     bool bad = false;  // last stage: the new state of the owned cell is not finite
+    const int cell = ty * TX + tx;
     if (own) {
         if (LATE && !FIRST) {
 #pragma unroll
-            for (int f = 0; f < 5; f++) v0[f] = V0[f * plane + gown];
+            for (int f = 0; f < 5; f++) v0[f] = own_tma ? sOwn[f * TC + cell] : V0[f * plane + gown];
         }
         double vk[5];  // the reference's Vk: this stage's input, or MUSCL-Hancock's carried working state
 #pragma unroll
@@ -549,7 +588,6 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
         }
         // flux divergence, GPU/Volume_kernel.cu:191-195
         const double invx = dt * P.inv_dx, invy = dt * P.inv_dy;
-        const int cell = ty * TX + tx;
 #pragma unroll
         for (int f = 0; f < 5; f++) {
             double FL = sFlux[(0 * 5 + f) * FS + cell], FR = sFlux[(1 * 5 + f) * FS + cell];
@@ -585,9 +623,15 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
         Vout[4 * plane + gown] = hc;
         if (LAST) {
             const double eps_h = P.eps_h;
-            if (h > eps_h) A.hmax[gown] = fmax(A.hmax[gown], h);
-            A.bmin[gown] = fmax(A.bmin[gown], z);
-            if (h > eps_h) A.eta_max[gown] = fmax(A.eta_max[gown], h - z);
+            if (own_tma) {
+                if (h > eps_h) A.hmax[gown] = fmax(sOwn[5 * TC + cell], h);
+                A.bmin[gown] = fmax(sOwn[6 * TC + cell], z);
+                if (h > eps_h) A.eta_max[gown] = fmax(sOwn[7 * TC + cell], h - z);
+            } else {
+                if (h > eps_h) A.hmax[gown] = fmax(A.hmax[gown], h);
+                A.bmin[gown] = fmax(A.bmin[gown], z);
+                if (h > eps_h) A.eta_max[gown] = fmax(A.eta_max[gown], h - z);
+            }
             double d = cfl_dt(P, h, qx, qy);
             if (!isnan(d)) dtcell = d;
             bad = !(finite64(h) && finite64(qx) && finite64(qy) && finite64(z) && finite64(hc));
@@ -740,24 +784,25 @@ EncodeTiledFn tensor_map_encoder() {
 namespace {
 
 struct Variant {
-    int tx, ty, nthr;
+    int tx, ty, nthr, own;
     size_t smem;
     // order2 stage0, order2 stage1, order1, MUSCL-Hancock order2, MUSCL-Hancock order1
     void (*k[5])(Stage64Args);
 };
 
-template <int TX, int TY, int MINB, int NTHR = TX * TY, bool LATE = false>
+template <int TX, int TY, int MINB, int NTHR = TX * TY, int OWN = 0>
 Variant make_variant() {
     Variant v;
     v.tx = TX;
     v.ty = TY;
     v.nthr = NTHR;
-    v.smem = Tile<TX, TY, NTHR>::smem();
-    v.k[0] = stage64_kernel<TX, TY, NTHR, MINB, 2, true, false, false, LATE>;
-    v.k[1] = stage64_kernel<TX, TY, NTHR, MINB, 2, false, true, false, LATE>;
-    v.k[2] = stage64_kernel<TX, TY, NTHR, MINB, 1, true, true, false, LATE>;
-    v.k[3] = stage64_kernel<TX, TY, NTHR, MINB, 2, true, true, true, LATE>;
-    v.k[4] = stage64_kernel<TX, TY, NTHR, MINB, 1, true, true, true, LATE>;
+    v.own = OWN;
+    v.smem = Tile<TX, TY, NTHR>::smem(OWN == 2);
+    v.k[0] = stage64_kernel<TX, TY, NTHR, MINB, 2, true, false, false, OWN>;
+    v.k[1] = stage64_kernel<TX, TY, NTHR, MINB, 2, false, true, false, OWN>;
+    v.k[2] = stage64_kernel<TX, TY, NTHR, MINB, 1, true, true, false, OWN>;
+    v.k[3] = stage64_kernel<TX, TY, NTHR, MINB, 2, true, true, true, OWN>;
+    v.k[4] = stage64_kernel<TX, TY, NTHR, MINB, 1, true, true, true, OWN>;
     return v;
 }
 
@@ -772,7 +817,8 @@ const Variant &variant() {
         if (e && !std::strcmp(e, "32x8t288")) return make_variant<32, 8, 2, 288>();
         if (e && !std::strcmp(e, "32x8t352")) return make_variant<32, 8, 2, 352>();
         if (e && !std::strcmp(e, "32x8t384")) return make_variant<32, 8, 2, 384>();
-        if (e && !std::strcmp(e, "32x8t320late")) return make_variant<32, 8, 2, 320, true>();
+        if (e && !std::strcmp(e, "32x8t320late")) return make_variant<32, 8, 2, 320, 1>();
+        if (e && !std::strcmp(e, "32x8t320own")) return make_variant<32, 8, 2, 320, 2>();
         // default: 32 x 8 tile, 320 threads, 2 CTAs per SM (shared memory
         // allows 2; 20 warps per SM at 96 registers, no spills).  Measured at
         // 4096^2: 256 threads 2161, 288 2308, 320 2514, 352 2365, 384 2331
@@ -795,14 +841,17 @@ cudaError_t stage64_prepare() {
     return cudaSuccess;
 }
 
-bool stage64_tma_maps(const double *bufA, const double *bufB, const unsigned char *mask, long long pitch, long long plane,
-                      int npx, int npy, CUtensorMap *tmA, CUtensorMap *tmB, CUtensorMap *tmM) {
+bool stage64_tma_maps(const double *bufA, const double *bufB, const unsigned char *mask, const double *const ext[3],
+                      long long pitch, long long plane, int npx, int npy, CUtensorMap *tmA, CUtensorMap *tmB,
+                      CUtensorMap *tmM, CUtensorMap *tmO, CUtensorMap tmE[3]) {
     EncodeTiledFn f = tensor_map_encoder();
     const Variant &v = variant();
     if (!f || npx < v.tx + 4 || npy < v.ty + 4) return false;
     if (reinterpret_cast<uintptr_t>(bufA) % 16 || reinterpret_cast<uintptr_t>(bufB) % 16 ||
         reinterpret_cast<uintptr_t>(mask) % 16 || pitch % 16)
         return false;
+    for (int k = 0; k < 3; k++)
+        if (reinterpret_cast<uintptr_t>(ext[k]) % 16) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)npx, (cuuint64_t)npy, 5};
     const cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(double), (cuuint64_t)plane * sizeof(double)};
     const cuuint32_t box[3] = {(cuuint32_t)(v.tx + 4), (cuuint32_t)(v.ty + 4), 5};
@@ -821,6 +870,16 @@ bool stage64_tma_maps(const double *bufA, const double *bufB, const unsigned cha
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return false;
+    const cuuint32_t obox[3] = {(cuuint32_t)v.tx, (cuuint32_t)v.ty, 5};
+    if (f(tmO, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(bufA), dims, strides, obox, es,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    for (int k = 0; k < 3; k++)
+        if (f(&tmE[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(ext[k]), dims, strides, obox, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
     return true;
 }
 

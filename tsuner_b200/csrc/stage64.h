@@ -43,6 +43,10 @@ struct Stage64Args {
     // inside the grid when `tma` is set
     CUtensorMap tmA, tmB;
     CUtensorMap tmM;  // the uint8 mask [npy][pitch] (box origin x0 - 16)
+    // boxes of the owned cells (TX x TY): U^n in bufA [5][npy][npx] and the
+    // running extrema hmax, bmin, eta_max [npy][npx]
+    CUtensorMap tmO;
+    CUtensorMap tmE[3];
     int tma;
     double *bufA;           // U^n at step entry (and U^{n+1} at exit, order 2)
     double *bufB;           // U* (order 2) / ping-pong partner (order 1, MUSCL-Hancock)
@@ -87,7 +91,10 @@ constexpr unsigned long long kDefaultWaitNs = 500000000ull;  // async.cuh kWaitN
 // encodes the TMA descriptors of the two FP64 state buffers for the current
 // tile shape; false if the driver cannot (the kernels then load with
 // ordinary instructions)
-bool stage64_tma_maps(const double *bufA, const double *bufB, const unsigned char *mask, long long pitch, long long plane,
-                      int npx, int npy, CUtensorMap *tmA, CUtensorMap *tmB, CUtensorMap *tmM);
+// (tmO, tmE[3]: the owned-cell boxes of bufA and of the extrema hmax, bmin,
+// eta_max)
+bool stage64_tma_maps(const double *bufA, const double *bufB, const unsigned char *mask, const double *const ext[3],
+                      long long pitch, long long plane, int npx, int npy, CUtensorMap *tmA, CUtensorMap *tmB,
+                      CUtensorMap *tmM, CUtensorMap *tmO, CUtensorMap tmE[3]);
 
 }  // namespace tsu
