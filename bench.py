@@ -509,7 +509,7 @@ def run_corrector(a, rank, world, local, dist):
     t_truth = time.perf_counter() - t0
     c = K.Corrector(n, n, f, max_batch=8, device=local)
     c.set_site(site.H)
-    c.set_options(a.corr_wbig, a.corr_clip)
+    c.set_options(a.corr_wbig, a.corr_clip, a.corr_envelope)
     c.add_samples(coarse_train, fine_train)
     c.add_samples(coarse_test, truth)
     # step-wise decay: half the steps at 1e-3, a quarter at 3e-4, a quarter at 1e-4
@@ -548,6 +548,7 @@ def run_corrector(a, rank, world, local, dist):
                    "network": "6 x conv3x3 32 ch, BF16 weights/activations, FP32 accumulate (tcgen05, TMEM)",
                    "train": {"iters": a.corr_iters, "batch": 8, "lr": "1e-3 / 3e-4 / 1e-4 (1/2, 1/4, 1/4 of the steps)",
                              "large_residual_weight": a.corr_wbig, "clip_depth": bool(a.corr_clip),
+                             "envelope": a.corr_envelope,
                              "ms": round(train_ms, 1),
                              "convs": convs, "loss_first": float(loss[:5].mean()),
                              "loss_last": float(loss[-10:].mean())},
@@ -698,6 +699,8 @@ def main():
                     help="corrector: loss weight 1 + w t^2 on large maximum-depth residuals")
     ap.add_argument("--corr-clip", type=int, default=0, choices=[0, 1],
                     help="corrector: clip the corrected maximum depth at 0")
+    ap.add_argument("--corr-envelope", type=float, default=0.0,
+                    help="corrector: clamp residuals to k x the training pairs' per-pixel envelope (0 = off)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     a.config3_steps = max(a.config3_steps, 10)

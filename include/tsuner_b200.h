@@ -308,13 +308,16 @@ int tsu_corr_set_weights(TsuCorrector *c, const float *W, const float *B);
 /* iters Adam steps on seeded mini-batches of samples [0, ntrain); loss[iters] (optional) */
 int tsu_corr_train(TsuCorrector *c, int ntrain, int iters, int batch, float lr, unsigned long long seed,
                    float *loss);
-/* Training and prediction options (defaults 0, 0).  large_residual_weight w
- * (>= 0) weights each pixel's maximum-depth term of the loss by 1 + w * t^2,
- * t = that pixel's normalised target residual, so that the few large
- * residuals at run-up fronts count for more than their share of pixels;
- * clip_depth = 1 clips the corrected maximum depth at 0 (a maximum depth is
- * never negative).  TSU_ERR_INVALID for w < 0 or clip_depth not 0/1. */
-int tsu_corr_set_options(TsuCorrector *c, float large_residual_weight, int clip_depth);
+/* Training and prediction options (defaults 0, 0, 0).  large_residual_weight
+ * w (>= 0) weights each pixel's maximum-depth term of the loss by
+ * 1 + w * t^2, t = that pixel's normalised target residual, so that the few
+ * large residuals at run-up fronts count for more than their share of
+ * pixels; clip_depth = 1 clips the corrected maximum depth at 0 (a maximum
+ * depth is never negative); envelope k > 0 clamps each predicted residual to
+ * k times the largest one that the training pairs of the last
+ * tsu_corr_train call needed at that pixel.  TSU_ERR_INVALID for w < 0,
+ * clip_depth not 0/1 or k < 0. */
+int tsu_corr_set_options(TsuCorrector *c, float large_residual_weight, int clip_depth, float envelope);
 /* corrected maps of samples [first, first+n): [n][ny][nx] each; base_* (optional) = interpolation only */
 int tsu_corr_predict(TsuCorrector *c, int first, int n, float *out_hmax, float *out_db, float *base_hmax,
                      float *base_db);

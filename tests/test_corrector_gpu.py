@@ -191,9 +191,38 @@ def test_options_weight_large_residuals_and_clip_depth():
             c.close()
     # same weights and batch at the first step: the weighted loss is larger
     assert first[1] > first[0], first
+
+
+def test_envelope_clamps_residuals_to_the_training_envelope():
+    """envelope k: each predicted residual lies within k times the largest
+    residual the training targets hold at that pixel (here computed on the
+    host from the same targets)."""
+    dev()
+    ny, f = 64, 4
+    Hf, coarse, fine = synthetic_samples(8, ny, f, 8)
+    c = K.Corrector(ny, ny, f, max_batch=4, seed=5)
+    try:
+        c.set_site(Hf)
+        c.add_samples(coarse, fine)
+        c.train(ntrain=6, iters=60, batch=4, lr=3e-3, seed=2)
+        oh, ob, bh, bb = c.predict(6, 2)
+        _, _, th, tb = c.predict(0, 6)   # the interpolation of the training samples
+        env_h = np.abs(fine[:6, 0] - th).max(axis=0)
+        env_b = np.abs(fine[:6, 1] - tb).max(axis=0)
+        for k in (0.5, 1.0):
+            c.set_options(0.0, False, k)
+            ch, cb, bh2, bb2 = c.predict(6, 2)
+            assert np.array_equal(bh2, bh) and np.array_equal(bb2, bb)
+            # float32 normalisation of the residuals: a few ulp of slack
+            assert (np.abs(ch - bh) <= k * env_h * (1 + 1e-5) + 1e-5).all()
+            assert (np.abs(cb - bb) <= k * env_b * (1 + 1e-5) + 1e-6).all()
+            inside = np.abs(oh - bh) < 0.9 * k * env_h  # unclamped residuals inside the envelope stay
+            assert np.allclose(ch[inside], oh[inside], rtol=0, atol=1e-5)
+    finally:
+        c.close()
     c = K.Corrector(ny, ny, f, max_batch=4, seed=3)
     try:
-        for bad in ((-1.0, 0), (0.0, 2)):
+        for bad in ((-1.0, 0, 0.0), (0.0, 2, 0.0), (0.0, 0, -1.0)):
             assert T.lib().tsu_corr_set_options(c._h, *bad) != 0
     finally:
         c.close()

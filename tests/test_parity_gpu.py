@@ -185,8 +185,44 @@ def test_steps_are_graph_chunk_independent():
     assert np.array_equal(a["V"], V)
 
 
+_VARIANT_RUN = """
+import sys, numpy as np
+import tsuner_b200 as T
+from tsuner_b200 import workloads as W
+w = W.nwave_shelf(300, 200, 10.0, slr=0.5, amp=2.0, period=200.0, t_series=200.0)
+s = T.solver_for(w)
+s.step(30)
+hm, bm, em = s.extrema()
+np.savez(sys.argv[1], V=s.state(), hmax=hm, bmin=bm, eta_max=em, t=np.array(s.time()))
+s.close()
+"""
+
+
+@pytest.mark.parametrize("variant", ["32x8t320reg", "32x8t320late", "16x16", "32x8t256"])
+def test_kernel_variants_value_identical(variant, tmp_path):
+    """Every FP64 kernel variant (tile shape, threads, where U^n waits for
+    the update) gives the default variant's results value for value; the
+    variant is chosen once per process (TSU_TILE64), so each runs in its own."""
+    import os
+    import subprocess
+    import sys
+    outs = {}
+    for name, env_v in (("default", None), (variant, variant)):
+        env = dict(os.environ)
+        env.pop("TSU_TILE64", None)
+        if env_v:
+            env["TSU_TILE64"] = env_v
+        path = str(tmp_path / (name + ".npz"))
+        r = subprocess.run([sys.executable, "-c", _VARIANT_RUN, path], env=env, capture_output=True, text=True,
+                           timeout=300, cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs[name] = np.load(path)
+    for k in ("V", "hmax", "bmin", "eta_max", "t"):
+        assert np.array_equal(outs["default"][k], outs[variant][k]), k
+
+
 # ------------------------------------------------ vs the reference CUDA build
-need_ref = pytest.mark.skipif(not oracle.ref_available("default"), reason="oracle/_ref not built")
+need_ref =pytest.mark.skipif(not oracle.ref_available("default"), reason="oracle/_ref not built")
 
 
 def ref_vs_new(w, nsteps, variant, sw, recipe_tol=REL_TOL):

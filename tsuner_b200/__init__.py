@@ -70,7 +70,7 @@ _ENS_SIG = {
     "tsu_corr_set_weights": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "tsu_corr_train": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_ulonglong, C.c_void_p], C.c_int),
     "tsu_corr_predict": ([C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 4, C.c_int),
-    "tsu_corr_set_options": ([C.c_void_p, C.c_float, C.c_int], C.c_int),
+    "tsu_corr_set_options": ([C.c_void_p, C.c_float, C.c_int, C.c_float], C.c_int),
     "tsu_corr_bench_conv": ([C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "tsu_corr_last_train_ms": ([C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)], C.c_int),
     "tsu_corr_conv3x3": ([C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,

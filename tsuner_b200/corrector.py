@@ -87,8 +87,8 @@ class Corrector:
         _ck(lib().tsu_corr_train(self._h, ntrain, iters, batch, lr, seed, _fp(loss)), "tsu_corr_train")
         return loss[:iters]
 
-    def set_options(self, large_residual_weight=0.0, clip_depth=False):
-        _ck(lib().tsu_corr_set_options(self._h, float(large_residual_weight), int(bool(clip_depth))),
+    def set_options(self, large_residual_weight=0.0, clip_depth=False, envelope=0.0):
+        _ck(lib().tsu_corr_set_options(self._h, float(large_residual_weight), int(bool(clip_depth)), float(envelope)),
             "tsu_corr_set_options")
 
     def predict(self, first, n):

@@ -676,15 +676,36 @@ __global__ void adam_kernel(float *__restrict__ Wm, float *__restrict__ mW, floa
     }
 }
 
-// corrected fields: base + scale * output channel; a maximum depth is not
-// negative (0 = never wet), so the corrected one is clipped at 0 when asked
+// Per-pixel envelope of the training targets: E[c][p] = max over the batch
+// (and earlier batches) of |T[b][p][c]|.  Non-negative floats order like
+// their bit patterns, so the maximum is an integer atomicMax.
+__global__ void envelope_kernel(const float *__restrict__ T, int nb, long long npix, float *__restrict__ E) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nb * npix;
+         g += (long long)gridDim.x * blockDim.x) {
+        const long long p = g % npix;
+        atomicMax(reinterpret_cast<int *>(E) + p, __float_as_int(fabsf(T[g * 2])));
+        atomicMax(reinterpret_cast<int *>(E) + npix + p, __float_as_int(fabsf(T[g * 2 + 1])));
+    }
+}
+
+// corrected fields: base + scale * output channel.  With an envelope E, each
+// channel's residual is first clamped to +-k E[c][p], k times the largest
+// residual the training pairs needed at that pixel.  A maximum depth is not
+// negative (0 = never wet), so the corrected one is clipped at 0 when asked.
 __global__ void apply_kernel(const float *__restrict__ Y, const float *__restrict__ base, long long npix,
-                             int clip_depth, float *__restrict__ out_h, float *__restrict__ out_b) {
+                             int clip_depth, const float *__restrict__ E, float k, float *__restrict__ out_h,
+                             float *__restrict__ out_b) {
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
          p += (long long)gridDim.x * blockDim.x) {
-        const float hc = base[p * 2] + kSh * Y[p * C];
+        float y0 = Y[p * C], y1 = Y[p * C + 1];
+        if (E) {
+            const float e0 = k * E[p], e1 = k * E[npix + p];
+            y0 = fminf(fmaxf(y0, -e0), e0);
+            y1 = fminf(fmaxf(y1, -e1), e1);
+        }
+        const float hc = base[p * 2] + kSh * y0;
         out_h[p] = clip_depth ? fmaxf(hc, 0.f) : hc;
-        out_b[p] = base[p * 2 + 1] + kSb * Y[p * C + 1];
+        out_b[p] = base[p * 2 + 1] + kSb * y1;
     }
 }
 
@@ -807,6 +828,11 @@ struct TsuCorrector {
     // options (tsu_corr_set_options)
     float wbig = 0.f;
     int clip_depth = 0;
+    float envelope = 0.f;
+    // per-pixel envelope of the normalised residual targets of samples
+    // [0, env_n) ([2][H*W]); ntrain = the training set of the last tsu_corr_train
+    float *E = nullptr;
+    int env_n = 0, ntrain = 0;
 };
 
 namespace {
@@ -829,7 +855,8 @@ uint64_t splitmix(uint64_t &s) {
 double uniform01(uint64_t &s) { return (double)(splitmix(s) >> 11) * (1.0 / 9007199254740992.0); }
 
 void free_all(TsuCorrector *c) {
-    float *fp[] = {c->Wm, c->mW, c->vW, c->gW, c->Bm, c->mB, c->vB, c->gB, c->Yout, c->T, c->base, c->Hf, c->coarse, c->fine};
+    float *fp[] = {c->Wm, c->mW, c->vW, c->gW, c->Bm, c->mB, c->vB, c->gB, c->Yout, c->T, c->base, c->Hf, c->coarse, c->fine,
+                   c->E};
     for (float *p : fp) cudaFree(p);
     cudaFree(c->Wbf);
     cudaFree(c->Wt);
@@ -909,6 +936,23 @@ int load_batch(TsuCorrector *c, const int *idx, int nb, bool targets) {
     CCK(cudaGetLastError());
     return TSU_OK;
 }
+
+// the residual envelope of training samples [0, n)
+int compute_envelope(TsuCorrector *c, int n) {
+    const long long npix = (long long)c->H * c->W;
+    CCK(cudaMemsetAsync(c->E, 0, 2 * npix * sizeof(float), c->st));
+    std::vector<int> idx(c->max_batch);
+    for (int s0 = 0; s0 < n; s0 += c->max_batch) {
+        const int nb = std::min(c->max_batch, n - s0);
+        for (int b = 0; b < nb; b++) idx[b] = s0 + b;
+        const int rc = load_batch(c, idx.data(), nb, true);
+        if (rc) return rc;
+        envelope_kernel<<<4 * num_sms(), 256, 0, c->st>>>(c->T, nb, npix, c->E);
+        CCK(cudaGetLastError());
+    }
+    c->env_n = n;
+    return TSU_OK;
+}
 }  // namespace
 
 extern "C" int tsu_corr_create(TsuCorrector **out, int ny, int nx, int factor, int max_batch, unsigned long long seed,
@@ -952,6 +996,7 @@ extern "C" int tsu_corr_create(TsuCorrector **out, int ny, int nx, int factor, i
     CAL(c->d_idx, (size_t)max_batch * 4);
     CAL(c->d_loss, 8);
     CAL(c->Hf, (size_t)ny * nx * 4);
+    CAL(c->E, (size_t)2 * ny * nx * 4);
 #undef CAL
     if (e == cudaSuccess) e = prepare();
     if (e != cudaSuccess) {
@@ -1037,10 +1082,12 @@ extern "C" int tsu_corr_num_samples(TsuCorrector *c, int *n) {
     return TSU_OK;
 }
 
-extern "C" int tsu_corr_set_options(TsuCorrector *c, float large_residual_weight, int clip_depth) {
-    if (!c || !(large_residual_weight >= 0.f) || (clip_depth != 0 && clip_depth != 1)) return TSU_ERR_INVALID;
+extern "C" int tsu_corr_set_options(TsuCorrector *c, float large_residual_weight, int clip_depth, float envelope) {
+    if (!c || !(large_residual_weight >= 0.f) || (clip_depth != 0 && clip_depth != 1) || !(envelope >= 0.f))
+        return TSU_ERR_INVALID;
     c->wbig = large_residual_weight;
     c->clip_depth = clip_depth;
+    c->envelope = envelope;
     return TSU_OK;
 }
 
@@ -1065,6 +1112,7 @@ extern "C" int tsu_corr_train(TsuCorrector *c, int ntrain, int iters, int batch,
     if (!c || ntrain < 1 || ntrain > c->nsamples || iters < 0 || batch < 1 || batch > c->max_batch)
         return TSU_ERR_INVALID;
     CCK(cudaSetDevice(c->device));
+    c->ntrain = ntrain;
     const int L = TsuCorrector::L;
     const size_t nw = (size_t)L * 32 * KROWS;
     const long long npix = (long long)batch * c->H * c->W;
@@ -1139,6 +1187,12 @@ extern "C" int tsu_corr_predict(TsuCorrector *c, int first, int n, float *out_hm
     if (!c || first < 0 || n < 1 || first + n > c->nsamples || !out_hmax || !out_db) return TSU_ERR_INVALID;
     CCK(cudaSetDevice(c->device));
     const size_t np = (size_t)c->H * c->W;
+    // the envelope clamp needs the training set's targets (none before training)
+    const bool clamp = c->envelope > 0.f && c->ntrain > 0;
+    if (clamp && c->env_n != c->ntrain) {
+        const int r = compute_envelope(c, c->ntrain);
+        if (r) return r;
+    }
     float *d_out = nullptr;
     CCK(cudaMalloc((void **)&d_out, 2 * np * 4));
     std::vector<float> bb(2 * np);
@@ -1148,8 +1202,8 @@ extern "C" int tsu_corr_predict(TsuCorrector *c, int first, int n, float *out_hm
         rc = load_batch(c, &s, 1, false);
         if (!rc) rc = forward(c, 1);
         if (rc) break;
-        apply_kernel<<<2 * num_sms(), 256, 0, c->st>>>(c->Yout, c->base, (long long)np, c->clip_depth, d_out,
-                                                         d_out + np);
+        apply_kernel<<<2 * num_sms(), 256, 0, c->st>>>(c->Yout, c->base, (long long)np, c->clip_depth,
+                                                         clamp ? c->E : nullptr, c->envelope, d_out, d_out + np);
         void *outs[2] = {out_hmax + k * np, out_db + k * np};
         const void *ins[2] = {d_out, d_out + np};
         if (cudaGetLastError() != cudaSuccess ||

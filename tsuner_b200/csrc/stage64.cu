@@ -817,13 +817,16 @@ const Variant &variant() {
         if (e && !std::strcmp(e, "32x8t288")) return make_variant<32, 8, 2, 288>();
         if (e && !std::strcmp(e, "32x8t352")) return make_variant<32, 8, 2, 352>();
         if (e && !std::strcmp(e, "32x8t384")) return make_variant<32, 8, 2, 384>();
+        if (e && !std::strcmp(e, "32x8t320reg")) return make_variant<32, 8, 2, 320, 0>();
         if (e && !std::strcmp(e, "32x8t320late")) return make_variant<32, 8, 2, 320, 1>();
-        if (e && !std::strcmp(e, "32x8t320own")) return make_variant<32, 8, 2, 320, 2>();
         // default: 32 x 8 tile, 320 threads, 2 CTAs per SM (shared memory
-        // allows 2; 20 warps per SM at 96 registers, no spills).  Measured at
-        // 4096^2: 256 threads 2161, 288 2308, 320 2514, 352 2365, 384 2331
-        // Mcell-steps/s; every choice is value-identical.
-        return make_variant<32, 8, 2, 320>();
+        // allows 2; 20 warps per SM at 92-96 registers, no spills), the
+        // second stage's U^n and extrema staged by TMA (OWN = 2, 107 KB of
+        // shared memory per CTA).  Measured at 4096^2: 256 threads 2161, 288
+        // 2308, 320 2514, 352 2365, 384 2331 Mcell-steps/s; with 320 threads
+        // OWN = 0 / 1 / 2: 2533 / 2566 / 2585 (one box, 100 steps).  Every
+        // choice is value-identical.
+        return make_variant<32, 8, 2, 320, 2>();
     }();
     return v;
 }
