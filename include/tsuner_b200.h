@@ -292,6 +292,9 @@ int tsu_ens_run_until(TsuEnsemble *e, double t_end, long max_steps, long *steps_
  * bed change, bathymetry; [3][ny/factor][nx/factor] per sample) plus the
  * fine bathymetry to fine-grid maximum depth and bed change [2][ny][nx]:
  * output = bilinear interpolation of the coarse maps + learned residual.
+ * Input channels: the interpolated maps, the fine bathymetry and its
+ * sub-grid detail, the coarse wet flag, a constant channel (marks the
+ * image border under the zero padding) and the pixel's column and row.
  * Trained with Adam on mean-square error against fine solves. */
 typedef struct TsuCorrector TsuCorrector;
 int tsu_corr_create(TsuCorrector **out, int ny, int nx, int factor, int max_batch, unsigned long long seed,

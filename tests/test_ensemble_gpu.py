@@ -114,3 +114,40 @@ def test_run_until_stops_each_member_at_its_end_time(reference_runs):
     e.sync()
     assert all(s.time()[2] == alone[k][1][2] + 1 for k, s in enumerate(e.members))
     e.close()
+
+
+def test_members_follow_the_fp64_plain_form(reference_runs):
+    """Each member of the ensemble against the same member in the FP64 plain
+    form (the reference's arithmetic) after the same simulated time: depth
+    within the FP32 form's run-up bound (2e-3 m, tests/test_fp32_gpu.py) and
+    the water volume within 1e-6 relative."""
+    from tsuner_b200.abi import make_switches
+    ws, _ = reference_runs
+    t_end = 8.0
+    e = make_ens(ws)
+    e.run_until(t_end)
+    e.sync()
+    try:
+        for k, w in enumerate(ws):
+            m = e.members[k]
+            V32, (t32, _, _) = m.state(), m.time()
+            sw64 = make_switches(order=w.sw.order, wbc=w.sw.wbc, read_files=w.sw.read_files, precision=0,
+                                 eta0=w.sw.eta0)
+            s = T.Solver(w.p, sw64)
+            try:
+                s.set_state(w.V)
+                s.set_mask(w.mask)
+                if w.sw.read_files:
+                    s.set_boundary_series(w.CC, w.tCC)
+                s.reset()
+                s.run_until(t_end)
+                V64, (t64, _, _) = s.state(), s.time()
+            finally:
+                s.close()
+            assert abs(t32 - t64) <= 1e-3 * t64
+            linf = np.abs(V32[0] - V64[0]).max()
+            assert linf <= 2e-3, (k, linf)
+            m32, m64 = V32[0].sum(), V64[0].sum()
+            assert abs(m32 - m64) <= 1e-6 * m64, (k, m32, m64)
+    finally:
+        e.close()

@@ -599,7 +599,12 @@ __global__ void features_kernel(const int *__restrict__ idx, int nb, const float
         const float Hfine = Hf[p];
         const int xi = min(x / f, wc - 1), yi = min(y / f, hc - 1);  // coarse cell containing the fine cell
         const float wet = cs[yi * wc + xi] > 0.f ? 1.f : 0.f;
-        const float v[8] = {hm / kSh, dbv / kSb, Hfine / kSH, (Hfine - Hc) / kSdH, wet, 0.f, 0.f, 0.f};
+        // channel 5 is 1 everywhere: the convolutions' zero padding turns it
+        // into a marker of the image border, where the other channels' padding
+        // would otherwise read as dry, flat land; 6 and 7 locate the pixel
+        // (the source enters through the west boundary)
+        const float v[8] = {hm / kSh, dbv / kSb, Hfine / kSH, (Hfine - Hc) / kSdH, wet, 1.f,
+                            (float)x / (float)max(W - 1, 1), (float)y / (float)max(H - 1, 1)};
         uint4 *d = reinterpret_cast<uint4 *>(X0 + g * C);
         d[0] = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
         d[1] = d[2] = d[3] = make_uint4(0, 0, 0, 0);
