@@ -695,11 +695,11 @@ def main():
     ap.add_argument("--corr-test", type=int, default=16, help="corrector: held-out sources")
     ap.add_argument("--corr-iters", type=int, default=400, help="corrector: Adam steps")
     ap.add_argument("--corr-tend", type=float, default=600.0, help="corrector: simulated seconds per source")
-    ap.add_argument("--corr-wbig", type=float, default=0.0,
+    ap.add_argument("--corr-wbig", type=float, default=16.0,
                     help="corrector: loss weight 1 + w t^2 on large maximum-depth residuals")
-    ap.add_argument("--corr-clip", type=int, default=0, choices=[0, 1],
+    ap.add_argument("--corr-clip", type=int, default=1, choices=[0, 1],
                     help="corrector: clip the corrected maximum depth at 0")
-    ap.add_argument("--corr-envelope", type=float, default=0.0,
+    ap.add_argument("--corr-envelope", type=float, default=1.0,
                     help="corrector: clamp residuals to k x the training pairs' per-pixel envelope (0 = off)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)

@@ -50,6 +50,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -80,6 +81,17 @@ constexpr int kFwdSmem = 1024 + kWBytes + kFwdBufs * kPatch + 64;
 constexpr int kFwdCtasPerSm = 4;  // 4 x (54 KB + 1 KB) of shared memory, 4 x 64 TMEM columns
 static_assert(kFwdCtasPerSm * (kFwdSmem + 1024) <= 228 * 1024 && kFwdCtasPerSm * 64 <= 512, "fwd residency");
 static_assert(kPlane % 128 == 0 && kPlane >= kPlaneData && kWBytes % 128 == 0, "TMA destinations");
+// warp-specialised forward (conv3x3_fwd_ws_kernel): warp 0 loads patches,
+// warp 1 issues the MMAs, warps 2-5 run the epilogue.  A ring of kWsBufs
+// patch buffers (full / empty barriers) and kWsAcc TMEM accumulators of 32
+// columns (full / empty barriers); the epilogue stages its output in a 2 KB
+// area per warp of its own.
+constexpr int kWsBufs = 6, kWsAcc = 4, kWsThreads = 192;
+constexpr int kWsStage = 4 * 2048;
+constexpr int kWsBarBytes = (2 * kWsBufs + 2 * kWsAcc) * 8 + 32;
+constexpr int kWsSmem = 1024 + kWBytes + kWsBufs * kPatch + kWsStage + kWsBarBytes;
+constexpr int kWsCtasPerSm = 2;  // 2 x (~98 KB + 1 KB) of shared memory, 2 x 128 TMEM columns
+static_assert(kWsCtasPerSm * (kWsSmem + 1024) <= 228 * 1024 && kWsCtasPerSm * 32 * kWsAcc <= 512, "ws residency");
 // wgrad: patch + dZ tile + A for half of the 8 K steps (4 x 3 M blocks x 4 KB);
 // ~67 KB, so three CTAs fit on an SM
 constexpr int kZPlane = 128 * 16;
@@ -131,6 +143,9 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t 
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 // thread `lane` of the warp receives TMEM lane (base + lane), 32 columns
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
@@ -206,7 +221,8 @@ struct ConvArgs {
 // goes the same way in two halves of 16 channels.  The gate is read per
 // pixel (staging it too measured slower: 131 vs 110 us per 8 x 512^2 launch).
 __device__ __forceinline__ void conv_epilogue(const ConvArgs &a, const TileGeom &G, int t, uint32_t taddr, int warp,
-                                              int lane, const float *sBias, unsigned char *stage) {
+                                              int lane, const float *sBias, unsigned char *stage,
+                                              uint64_t *release = nullptr) {
     const int img = t / G.per_img, r = t - img * G.per_img;
     const int tyi = r / G.ntx, txi = r - tyi * G.ntx;
     const int x0 = txi * TXP, y0 = tyi * TYP;
@@ -224,6 +240,11 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs &a, const TileGeom 
     }
     float acc[32];
     tmem_ld32(taddr + ((uint32_t)(warp * 32) << 16), acc);
+    if (release) {  // the accumulator is in registers: hand its TMEM columns back to the MMA issuer
+        fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(release);
+    }
 #pragma unroll
     for (int n = 0; n < 32; n++) {
         float v = acc[n] + sBias[n];
@@ -398,6 +419,145 @@ __global__ void __launch_bounds__(128) conv3x3_fwd_kernel(ConvArgs a, const __gr
     __syncthreads();
     fence_after();
     if (warp == 0) tmem_dealloc(tmem, 64);
+}
+
+// Warp-specialised forward convolution (same tiles, operands and epilogue as
+// conv3x3_fwd_kernel).  The CTA's tiles are t = blockIdx.x + k * gridDim.x.
+//   warp 0 (lane 0): tile k -> patch buffer k % kWsBufs once the MMAs of tile
+//     k - kWsBufs have released it (empty barrier), TMA, full barrier;
+//   warp 1 (lane 0): waits for the patch and for a free accumulator
+//     (tile k - kWsAcc's epilogue has read it), issues the 18 MMAs of tile k
+//     into accumulator k % kWsAcc and commits to the patch's empty barrier and
+//     the accumulator's full barrier;
+//   warps 2-5: wait for the accumulator, read their 32 TMEM lanes (warp w
+//     reads lanes 32 (w % 4) ..), release the accumulator, finish the tile.
+// No role waits at a CTA barrier inside the loop, so MMAs of tile k run
+// while tile k - 1's epilogue stores and tile k + 1..k + 5 load.  Every wait
+// is bounded; a role whose wait expires sets the error word and leaves its
+// loop, the others' waits then expire in turn, and before TMEM is freed the
+// producer waits for its issued-but-unconsumed patch loads and the MMA warp
+// for its last MMAs.
+__global__ void __launch_bounds__(kWsThreads) conv3x3_fwd_ws_kernel(ConvArgs a, const __grid_constant__ CUtensorMap tmX) {
+    extern __shared__ unsigned char sm_raw[];
+    unsigned char *sm = smem_align<1024>(sm_raw);
+    unsigned char *sW = sm;
+    unsigned char *sP0 = sm + kWBytes;                         // kWsBufs patch buffers
+    unsigned char *sStage = sP0 + kWsBufs * kPatch;            // 4 x 2 KB epilogue staging
+    uint64_t *full = reinterpret_cast<uint64_t *>(sStage + kWsStage);  // [kWsBufs] patch landed
+    uint64_t *empty = full + kWsBufs;                                  // [kWsBufs] patch's MMAs done
+    uint64_t *accf = empty + kWsBufs;                                  // [kWsAcc] accumulator ready
+    uint64_t *acce = accf + kWsAcc;                                    // [kWsAcc] accumulator read
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(acce + kWsAcc);
+    int *sCount = reinterpret_cast<int *>(tslot + 1);  // [0] loads issued, [1] patches consumed
+    __shared__ float sBias[32];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const TileGeom G = tile_geom(a.nimg, a.H, a.W);
+    const int ntile = (int)blockIdx.x < G.total ? (G.total - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    for (int c = tid; c < 32 * 36; c += kWsThreads) {
+        const int n = c / 36, r = c - n * 36;  // r = tap * 4 + quarter
+        cp_async16(sW + r * 512 + n * 16, a.Wk + n * KROWS + r * 8, 16);
+    }
+    cp_async_commit();
+    if (tid < 32) sBias[tid] = a.bias ? a.bias[tid] : 0.f;
+    if (warp == 1) tmem_alloc(tslot, 32 * kWsAcc);
+    if (tid == 0) {
+        for (int k = 0; k < kWsBufs; k++) {
+            mbar_init(&full[k], 1);
+            mbar_init(&empty[k], 1);
+        }
+        for (int k = 0; k < kWsAcc; k++) {
+            mbar_init(&accf[k], 1);
+            mbar_init(&acce[k], 4);  // one arrival per epilogue warp
+        }
+        sCount[0] = sCount[1] = 0;
+        mbar_init_fence();
+    }
+    cp_async_wait_all();
+    fence_async_smem();  // the weights, written by cp.async, are read by the MMAs (async proxy)
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int k = 0;
+            for (; k < ntile; k++) {
+                const int b = k % kWsBufs;
+                if (k >= kWsBufs && !mbar_wait_first(&empty[b], ((k / kWsBufs) - 1) & 1)) {
+                    atomicExch(&g_corr_err, 1);
+                    break;
+                }
+                const int t = (int)blockIdx.x + k * (int)gridDim.x;
+                const int img = t / G.per_img, r = t - img * G.per_img;
+                const int tyi = r / G.ntx, txi = r - tyi * G.ntx;
+                mbar_expect_tx(&full[b], 4 * kPlaneData);
+                issue_patch(&tmX, img, txi * TXP, tyi * TYP, sP0 + b * kPatch, &full[b]);
+            }
+            sCount[0] = k;
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t id = idesc(128, 32, 0, 0);
+            const uint32_t w_u32 = smem_u32(sW);
+            int k = 0;
+            for (; k < ntile; k++) {
+                const int b = k % kWsBufs, ac = k % kWsAcc;
+                if (!mbar_wait_first(&full[b], (k / kWsBufs) & 1)) {
+                    atomicExch(&g_corr_err, 1);
+                    break;
+                }
+                sCount[1] = k + 1;
+                if (k >= kWsAcc && !mbar_wait_first(&acce[ac], ((k / kWsAcc) - 1) & 1)) {
+                    atomicExch(&g_corr_err, 1);
+                    break;
+                }
+                fence_after();
+                const uint32_t p_u32 = smem_u32(sP0 + b * kPatch);
+                const uint32_t d = tmem + (uint32_t)(ac * 32);
+#pragma unroll 1
+                for (int tap = 0; tap < 9; tap++) {
+                    const int dy = tap / 3, dx = tap - dy * 3;
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const uint64_t da = sdesc(p_u32 + 2 * h * kPlane + (dy * PW + dx) * 16, kPlane, PW * 16);
+                        const uint64_t db = sdesc(w_u32 + (tap * 4 + 2 * h) * 512, 512, 128);
+                        mma_bf16(d, da, db, id, (tap | h) ? 1u : 0u);
+                    }
+                }
+                mma_commit(&empty[b]);
+                mma_commit(&accf[ac]);
+            }
+            // the MMAs issued last may still run: they signal the last
+            // accumulator's full barrier when done
+            if (k > 0) mbar_wait(&accf[(k - 1) % kWsAcc], ((k - 1) / kWsAcc) & 1);
+        }
+    } else {
+        const int q = warp & 3;  // TMEM lane quarter this warp may read
+        for (int k = 0; k < ntile; k++) {
+            const int ac = k % kWsAcc;
+            // every lane waits; the warp leaves together if any lane's wait
+            // expired (the TMEM load below is a warp-wide instruction)
+            const bool ok = mbar_wait_first(&accf[ac], (k / kWsAcc) & 1);
+            if (__any_sync(0xffffffffu, !ok)) {
+                if (lane == 0) atomicExch(&g_corr_err, 1);
+                break;
+            }
+            fence_after();
+            const int t = (int)blockIdx.x + k * (int)gridDim.x;
+            conv_epilogue(a, G, t, tmem + (uint32_t)(ac * 32), q, lane, sBias, sStage, &acce[ac]);
+        }
+    }
+    __syncwarp();
+    fence_before();
+    __syncthreads();
+    if (tid == 0) {  // patch loads issued but never consumed (an expired wait): let them land
+        for (int k = sCount[1]; k < sCount[0]; k++) mbar_wait(&full[k % kWsBufs], (k / kWsBufs) & 1);
+    }
+    __syncthreads();
+    fence_after();
+    if (warp == 1) tmem_dealloc(tmem, 32 * kWsAcc);
 }
 
 // Weight (and bias) gradient, accumulated into dW[cout][288] and db[32].
@@ -734,6 +894,8 @@ cudaError_t prepare() {
     if (done) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(conv3x3_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdSmem);
     if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(conv3x3_fwd_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmem);
+    if (e == cudaSuccess)
         e = cudaFuncSetAttribute(conv3x3_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem);
     if (e == cudaSuccess) done = true;
     return e;
@@ -749,6 +911,15 @@ int num_sms() {
     return n;
 }
 
+// TSU_CONV_FWD=ws selects the warp-specialised forward kernel
+bool fwd_ws() {
+    static const bool ws = [] {
+        const char *e = std::getenv("TSU_CONV_FWD");
+        return e && !std::strcmp(e, "ws");
+    }();
+    return ws;
+}
+
 cudaError_t conv_launch(const ConvArgs &a, cudaStream_t st) {
     cudaError_t e = prepare();
     if (e != cudaSuccess) return e;
@@ -757,6 +928,11 @@ cudaError_t conv_launch(const ConvArgs &a, cudaStream_t st) {
     e = make_map(&mx, a.X, a.nimg, a.H, a.W, PW, PH);
     if (e != cudaSuccess) return e;
     const TileGeom G = tile_geom(a.nimg, a.H, a.W);
+    if (fwd_ws()) {  // persistent CTAs, kWsCtasPerSm per SM
+        const int ctas = std::min(G.total, kWsCtasPerSm * num_sms());
+        conv3x3_fwd_ws_kernel<<<ctas, kWsThreads, kWsSmem, st>>>(a, mx);
+        return cudaGetLastError();
+    }
     // persistent CTAs, kFwdCtasPerSm per SM (shared memory and TMEM bound)
     const int ctas = std::min(G.total, kFwdCtasPerSm * num_sms());
     conv3x3_fwd_kernel<<<ctas, 128, kFwdSmem, st>>>(a, mx);
