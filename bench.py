@@ -496,7 +496,7 @@ def run_corrector(a, rank, world, local, dist):
     whole pipeline)."""
     from tsuner_b200 import corrector as K
     n, f, t_end = a.corr_fine, 4, a.corr_tend
-    site = K.make_site(n=n, factor=f)
+    site = K.make_site(n=n, factor=f, dx=a.corr_dx)
     train_src = K.make_sources(a.corr_train, seed=11)
     test_src = K.make_sources(a.corr_test, seed=12)
     t0 = time.perf_counter()
@@ -695,6 +695,7 @@ def main():
     ap.add_argument("--corr-test", type=int, default=16, help="corrector: held-out sources")
     ap.add_argument("--corr-iters", type=int, default=400, help="corrector: Adam steps")
     ap.add_argument("--corr-tend", type=float, default=600.0, help="corrector: simulated seconds per source")
+    ap.add_argument("--corr-dx", type=float, default=10.0, help="corrector: fine cell size (m)")
     ap.add_argument("--corr-wbig", type=float, default=16.0,
                     help="corrector: loss weight 1 + w t^2 on large maximum-depth residuals")
     ap.add_argument("--corr-clip", type=int, default=1, choices=[0, 1],

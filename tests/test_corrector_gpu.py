@@ -281,3 +281,39 @@ def test_held_out_sources_improve_on_interpolation():
     assert ew["hmax_rmse_m"] < e0["hmax_rmse_m"]
     assert ew["db_rmse_m"] < e0["db_rmse_m"]
     assert ew["hmax_linf_m"] <= 1.1 * e0["hmax_linf_m"]
+
+
+_PLAIN_RUN = """
+import sys, ctypes as C, numpy as np, torch
+import tsuner_b200 as T
+g = torch.Generator().manual_seed(21)
+X = torch.randn(3, 40, 72, 32, generator=g).to(torch.bfloat16).cuda()
+Wk = (torch.randn(32, 9, 32, generator=g) * 0.1).to(torch.bfloat16).cuda()
+b = (torch.randn(32, generator=g) * 0.1).cuda()
+Y = torch.zeros((3, 40, 72, 32), device="cuda", dtype=torch.float32)
+rc = T.lib().tsu_corr_conv3x3(C.c_void_p(X.data_ptr()), 3, 40, 72, C.c_void_p(Wk.data_ptr()),
+                              C.c_void_p(b.data_ptr()), 1, None, None, C.c_void_p(Y.data_ptr()), None)
+assert rc == 0 and T.lib().tsu_corr_status() == 0
+np.save(sys.argv[1], Y.cpu().numpy())
+"""
+
+
+def test_both_forward_kernels_give_identical_outputs(tmp_path):
+    """The warp-specialised forward kernel (default) and conv3x3_fwd_kernel
+    (TSU_CONV_FWD=plain) issue the same MMAs in the same order and share the
+    epilogue: their outputs are equal value for value.  The kernel is chosen
+    once per process, so each runs in its own."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = {}
+    for name in ("ws", "plain"):
+        env = dict(os.environ, TSU_CONV_FWD=name)
+        path = str(tmp_path / (name + ".npy"))
+        r = subprocess.run([sys.executable, "-c", _PLAIN_RUN, path], env=env, cwd=root, capture_output=True, text=True,
+                           timeout=300)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[name] = np.load(path)
+    assert np.abs(out["ws"]).max() > 0
+    assert np.array_equal(out["ws"], out["plain"])
