@@ -181,6 +181,20 @@ int tsu_set_boundary_series(TsuSolver *s, const double *CC, const double *tCC,
 /* Resets t = 0, the running extrema to -1e30 and computes the initial dt
  * (GPU/main_TSUNER.cu:142-149).  Must follow tsu_set_state. */
 int tsu_reset(TsuSolver *s);
+/* Resume from a checkpoint (no counterpart in the reference, whose NetCDF
+ * frames hold derived fields only).  A checkpoint is tsu_get_state,
+ * tsu_get_extrema and tsu_get_time of a run; to continue it: tsu_set_state
+ * (the saved state), tsu_set_mask, tsu_set_boundary_series, tsu_reset, then
+ * tsu_resume with the saved t, step count and extrema (any extrema pointer
+ * may be NULL: that field keeps the fresh -1e30).  The next dt is the one
+ * tsu_reset computed from the state: the dt the interrupted run would have
+ * taken (the same formula on the same state), so an FP64 run continues value
+ * for value.  The FP32 form stores surface deviations, which come back
+ * through the FP64 state and may then differ in the last float bit;
+ * MUSCL-Hancock's working state restarts as the filtered state.
+ * TSU_ERR_INVALID before tsu_reset, for a slab, or for t < 0 / steps < 0. */
+int tsu_resume(TsuSolver *s, double t, long steps, const double *hmax, const double *bmin_rawH,
+               const double *eta_max);
 /* Enqueues nsteps time steps on the solver's stream (no host sync). */
 int tsu_step(TsuSolver *s, long nsteps);
 /* Steps while t < t_end (the reference loop condition), at most max_steps;

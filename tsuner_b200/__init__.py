@@ -27,7 +27,7 @@ EXPORTS = [
     "tsu_switches_default", "tsu_set_default_switches", "tsu_get_default_switches",
     "tsu_derive_params", "tsu_parse_data_dat",
     "tsu_create", "tsu_destroy", "tsu_set_state", "tsu_set_mask", "tsu_set_boundary_series",
-    "tsu_reset", "tsu_step", "tsu_run_until", "tsu_sync", "tsu_get_state", "tsu_get_extrema",
+    "tsu_reset", "tsu_resume", "tsu_step", "tsu_run_until", "tsu_sync", "tsu_get_state", "tsu_get_extrema",
     "tsu_get_time", "tsu_get_sums", "tsu_get_consts", "tsu_last_step_ms", "tsu_last_step_launches",
     "tsu_state_device", "tsu_cfl_dt_noalloc", "tsu_copy_planes_to_device", "tsu_copy_planes_to_host",
     "tsu_copy_bytes_to_device", "tsu_copy_bytes_to_host", "tsu_host_threads", "tsu_strerror", "tsu_last_error",
@@ -111,6 +111,7 @@ def lib():
             "tsu_set_mask": ([vp, vp], C.c_int),
             "tsu_set_boundary_series": ([vp, vp, vp, C.c_ulong], C.c_int),
             "tsu_reset": ([vp], C.c_int),
+            "tsu_resume": ([vp, C.c_double, C.c_long, vp, vp, vp], C.c_int),
             "tsu_step": ([vp, C.c_long], C.c_int),
             "tsu_run_until": ([vp, C.c_double, C.c_long, C.POINTER(C.c_long)], C.c_int),
             "tsu_sync": ([vp], C.c_int),
@@ -233,6 +234,14 @@ class Solver:
 
     def reset(self):
         _ck(lib().tsu_reset(self._h), "tsu_reset")
+
+    def resume(self, t, steps, extrema=None):
+        """Continue a checkpoint after set_state / set_mask / set_boundary_series
+        / reset: the saved (t, steps) of time() and optionally the saved
+        (hmax, bmin, eta_max) of extrema()."""
+        ex = [None] * 3 if extrema is None else [None if e is None else np.ascontiguousarray(e, np.float64)
+                                                 for e in extrema]
+        _ck(lib().tsu_resume(self._h, float(t), int(steps), *[_p(e) for e in ex]), "tsu_resume")
 
     def step(self, n):
         _ck(lib().tsu_step(self._h, n), "tsu_step")

@@ -555,6 +555,42 @@ extern "C" int tsu_reset(TsuSolver *s) {
     return TSU_OK;
 }
 
+// FP64 host planes -> the FP32 form's float extrema (exact for values that
+// came from float extrema)
+__global__ void narrow_kernel(const double *__restrict__ a, float *__restrict__ b, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+extern "C" int tsu_resume(TsuSolver *s, double t, long steps, const double *hmax, const double *bmin_rawH,
+                          const double *eta_max) {
+    if (!s || !s->ready || s->slab || steps < 0 || !(t >= 0.0) || !std::isfinite(t)) return TSU_ERR_INVALID;
+    CK(cudaSetDevice(s->device));
+    const double *src[3] = {hmax, bmin_rawH, eta_max};
+    void *ext[3] = {s->hmax, s->bmin, s->eta};
+    if (s->fp32) {
+        int r = staging(s);
+        if (r) return r;
+    }
+    for (int f = 0; f < 3; f++) {
+        if (!src[f]) continue;
+        double *d = s->fp32 ? s->stage64 + f * s->plane : (double *)ext[f];
+        void *dst[1] = {d + s->own_off()};
+        const void *from[1] = {src[f]};
+        CK(tsu::planes_h2d(1, dst, s->pitch * sizeof(double), from, s->p.npx * sizeof(double),
+                           s->p.npx * sizeof(double), s->p.npy, s->st));
+        if (s->fp32) {
+            narrow_kernel<<<1184, 256, 0, s->st>>>(d, (float *)ext[f], s->plane);
+            CK(cudaGetLastError());
+        }
+    }
+    const double ts[2] = {t, (double)steps};
+    CK(cudaMemcpyAsync(s->scal + SC_T, &ts[0], sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->scal + SC_STEPS, &ts[1], sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return TSU_OK;
+}
+
 int TsuSolver::launch_steps(long n) {
     if (fp32) {
         Stage32Args a = args32();
