@@ -307,8 +307,8 @@ int tsu_ens_run_until(TsuEnsemble *e, double t_end, long max_steps, long *steps_
  * fine bathymetry to fine-grid maximum depth and bed change [2][ny][nx]:
  * output = bilinear interpolation of the coarse maps + learned residual.
  * Input channels: the interpolated maps, the fine bathymetry and its
- * sub-grid detail, the coarse wet flag, a constant channel (marks the
- * image border under the zero padding) and the pixel's column and row.
+ * sub-grid detail, the coarse wet flag, a constant channel and the cell's
+ * column and row, on the fine grid padded by 8 cells of edge values.
  * Trained with Adam on mean-square error against fine solves. */
 typedef struct TsuCorrector TsuCorrector;
 int tsu_corr_create(TsuCorrector **out, int ny, int nx, int factor, int max_batch, unsigned long long seed,
@@ -338,7 +338,10 @@ int tsu_corr_set_options(TsuCorrector *c, float large_residual_weight, int clip_
 /* corrected maps of samples [first, first+n): [n][ny][nx] each; base_* (optional) = interpolation only */
 int tsu_corr_predict(TsuCorrector *c, int first, int n, float *out_hmax, float *out_db, float *base_hmax,
                      float *base_db);
-/* device time per forward convolution over nimg fine images and TFLOP/s */
+/* device time per forward convolution over nimg images and TFLOP/s (the
+ * network runs on the fine image padded by 8 cells on each side with its
+ * edge values, so that no fine cell sees the convolutions' zero padding;
+ * the FLOPs count the padded pixels) */
 int tsu_corr_bench_conv(TsuCorrector *c, int nimg, int iters, double *ms_per_conv, double *tflops);
 int tsu_corr_last_train_ms(TsuCorrector *c, double *ms, long *convs);
 /* Raw kernels on caller-owned device buffers (NHWC BF16, 32 channels):

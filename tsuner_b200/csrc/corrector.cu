@@ -738,19 +738,43 @@ __device__ __forceinline__ float up_bilinear(const float *__restrict__ p, int hc
     return (1.f - ay) * ((1.f - ax) * a + ax * b) + ay * ((1.f - ax) * c + ax * d);
 }
 
-// Builds the 32-channel BF16 input of sample idx[b] and, when targets are
-// requested, the normalised residual targets T[b][p][2].
+// The network runs on a canvas padded by kPad pixels on each side: a
+// padded pixel holds the features of the nearest fine cell (edge
+// replication), so that no fine cell is within the 6-layer network's
+// receptive radius (6 pixels) of the convolutions' zero padding, which would
+// otherwise read as dry, flat land at the image border.  Targets and the
+// loss cover the fine cells only.
+constexpr int kPad = 8;
+
+struct Canvas {
+    int H, W, Hp, Wp;  // fine image, padded canvas
+};
+__host__ __device__ inline Canvas canvas(int H, int W) { return Canvas{H, W, H + 2 * kPad, W + 2 * kPad}; }
+// padded pixel (xp, yp) -> its fine cell (x, y); true if it is that cell
+__device__ __forceinline__ bool unpad(const Canvas &cv, int xp, int yp, int &x, int &y) {
+    x = min(max(xp - kPad, 0), cv.W - 1);
+    y = min(max(yp - kPad, 0), cv.H - 1);
+    return x == xp - kPad && y == yp - kPad;
+}
+
+// Builds the 32-channel BF16 input of sample idx[b] on the padded canvas
+// and, when targets are requested, the normalised residual targets
+// T[b][pp][2] (0 outside the fine image); base[b][pp][2] = the interpolated
+// coarse maps.
 //   coarse: [nsamples][3][hc*wc] = maximum depth, bed change, bathymetry H
 //   fineT:  [nsamples][2][H*W]   = maximum depth, bed change (or null)
 __global__ void features_kernel(const int *__restrict__ idx, int nb, const float *__restrict__ coarse,
-                                const float *__restrict__ fineT, const float *__restrict__ Hf, int H, int W, int hc,
+                                const float *__restrict__ fineT, const float *__restrict__ Hf, Canvas cv, int hc,
                                 int wc, int f, bf16 *__restrict__ X0, float *__restrict__ T, float *__restrict__ base) {
-    const long long npix = (long long)H * W;
-    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nb * npix;
+    const long long npix = (long long)cv.H * cv.W, nppx = (long long)cv.Hp * cv.Wp;
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nb * nppx;
          g += (long long)gridDim.x * blockDim.x) {
-        const int b = (int)(g / npix);
-        const long long p = g - (long long)b * npix;
-        const int y = (int)(p / W), x = (int)(p - (long long)y * W);
+        const int b = (int)(g / nppx);
+        const long long pp = g - (long long)b * nppx;
+        const int yp = (int)(pp / cv.Wp), xp = (int)(pp - (long long)yp * cv.Wp);
+        int x, y;
+        const bool inside = unpad(cv, xp, yp, x, y);
+        const long long p = (long long)y * cv.W + x;
         const int s = idx[b];
         const float *cs = coarse + (long long)s * 3 * hc * wc;
         const float hm = up_bilinear(cs, hc, wc, f, x, y);
@@ -759,12 +783,10 @@ __global__ void features_kernel(const int *__restrict__ idx, int nb, const float
         const float Hfine = Hf[p];
         const int xi = min(x / f, wc - 1), yi = min(y / f, hc - 1);  // coarse cell containing the fine cell
         const float wet = cs[yi * wc + xi] > 0.f ? 1.f : 0.f;
-        // channel 5 is 1 everywhere: the convolutions' zero padding turns it
-        // into a marker of the image border, where the other channels' padding
-        // would otherwise read as dry, flat land; 6 and 7 locate the pixel
+        // channel 5 is 1 everywhere (a bias input); 6 and 7 locate the cell
         // (the source enters through the west boundary)
         const float v[8] = {hm / kSh, dbv / kSb, Hfine / kSH, (Hfine - Hc) / kSdH, wet, 1.f,
-                            (float)x / (float)max(W - 1, 1), (float)y / (float)max(H - 1, 1)};
+                            (float)x / (float)max(cv.W - 1, 1), (float)y / (float)max(cv.H - 1, 1)};
         uint4 *d = reinterpret_cast<uint4 *>(X0 + g * C);
         d[0] = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
         d[1] = d[2] = d[3] = make_uint4(0, 0, 0, 0);
@@ -774,31 +796,39 @@ __global__ void features_kernel(const int *__restrict__ idx, int nb, const float
         }
         if (T && fineT) {
             const float *ft = fineT + (long long)s * 2 * npix;
-            T[g * 2] = (ft[p] - hm) / kSh;
-            T[g * 2 + 1] = (ft[npix + p] - dbv) / kSb;
+            T[g * 2] = inside ? (ft[p] - hm) / kSh : 0.f;
+            T[g * 2 + 1] = inside ? (ft[npix + p] - dbv) / kSb : 0.f;
         }
     }
 }
 
-// Mean-square loss over the 2 output channels, each pixel's maximum-depth
-// term weighted by 1 + wbig * T^2 (T: the normalised residual target), so
-// that the few large residuals at run-up fronts weigh more than their share
-// of pixels; dY = d(loss)/d(output) in BF16 (channels 2..31 zero); loss sum
-// accumulated in FP64.
-__global__ void loss_kernel(const float *__restrict__ Y, const float *__restrict__ T, long long npix, float wbig,
+// Mean-square loss over the 2 output channels of the fine cells, each
+// cell's maximum-depth term weighted by 1 + wbig * T^2 (T: the normalised
+// residual target), so that the few large residuals at run-up fronts weigh
+// more than their share of cells; dY = d(loss)/d(output) in BF16 (channels
+// 2..31 and the padding zero); loss sum accumulated in FP64.
+__global__ void loss_kernel(const float *__restrict__ Y, const float *__restrict__ T, int nb, Canvas cv, float wbig,
                             bf16 *__restrict__ dY, double *__restrict__ loss) {
     __shared__ double sred[32];
-    const float scale = 1.f / (float)npix;  // d/dy of sum(w d^2) / (2 npix)
+    const long long nppx = (long long)cv.Hp * cv.Wp;
+    const float scale = 1.f / (float)((long long)nb * cv.H * cv.W);  // d/dy of sum(w d^2) / (2 cells)
     double acc = 0.0;
-    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
-         p += (long long)gridDim.x * blockDim.x) {
-        const float t0 = T[p * 2];
-        const float w0 = 1.f + wbig * t0 * t0;
-        const float d0 = Y[p * C] - t0, d1 = Y[p * C + 1] - T[p * 2 + 1];
-        acc += (double)w0 * d0 * d0 + (double)d1 * d1;
-        uint4 *g = reinterpret_cast<uint4 *>(dY + p * C);
-        g[0] = make_uint4(pack2(scale * w0 * d0, scale * d1), 0, 0, 0);
-        g[1] = g[2] = g[3] = make_uint4(0, 0, 0, 0);
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nb * nppx;
+         g += (long long)gridDim.x * blockDim.x) {
+        const long long pp = g % nppx;
+        const int yp = (int)(pp / cv.Wp), xp = (int)(pp - (long long)yp * cv.Wp);
+        int x, y;
+        float d0 = 0.f, d1 = 0.f, w0 = 0.f;
+        if (unpad(cv, xp, yp, x, y)) {
+            const float t0 = T[g * 2];
+            w0 = 1.f + wbig * t0 * t0;
+            d0 = Y[g * C] - t0;
+            d1 = Y[g * C + 1] - T[g * 2 + 1];
+            acc += (double)w0 * d0 * d0 + (double)d1 * d1;
+        }
+        uint4 *gp = reinterpret_cast<uint4 *>(dY + g * C);
+        gp[0] = make_uint4(pack2(scale * w0 * d0, scale * d1), 0, 0, 0);
+        gp[1] = gp[2] = gp[3] = make_uint4(0, 0, 0, 0);
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = acc;
@@ -841,36 +871,48 @@ __global__ void adam_kernel(float *__restrict__ Wm, float *__restrict__ mW, floa
     }
 }
 
-// Per-pixel envelope of the training targets: E[c][p] = max over the batch
-// (and earlier batches) of |T[b][p][c]|.  Non-negative floats order like
-// their bit patterns, so the maximum is an integer atomicMax.
-__global__ void envelope_kernel(const float *__restrict__ T, int nb, long long npix, float *__restrict__ E) {
+// Per-cell envelope of the training targets: E[c][p] = max over the batch
+// (and earlier batches) of |T[b][p][c]| over the fine cells p.  Non-negative
+// floats order like their bit patterns, so the maximum is an integer
+// atomicMax.
+__global__ void envelope_kernel(const float *__restrict__ T, int nb, Canvas cv, float *__restrict__ E) {
+    const long long npix = (long long)cv.H * cv.W;
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < nb * npix;
          g += (long long)gridDim.x * blockDim.x) {
-        const long long p = g % npix;
-        atomicMax(reinterpret_cast<int *>(E) + p, __float_as_int(fabsf(T[g * 2])));
-        atomicMax(reinterpret_cast<int *>(E) + npix + p, __float_as_int(fabsf(T[g * 2 + 1])));
+        const int b = (int)(g / npix);
+        const long long p = g - (long long)b * npix;
+        const int y = (int)(p / cv.W), x = (int)(p - (long long)y * cv.W);
+        const long long gp = (long long)b * cv.Hp * cv.Wp + (long long)(y + kPad) * cv.Wp + (x + kPad);
+        atomicMax(reinterpret_cast<int *>(E) + p, __float_as_int(fabsf(T[gp * 2])));
+        atomicMax(reinterpret_cast<int *>(E) + npix + p, __float_as_int(fabsf(T[gp * 2 + 1])));
     }
 }
 
-// corrected fields: base + scale * output channel.  With an envelope E, each
-// channel's residual is first clamped to +-k E[c][p], k times the largest
-// residual the training pairs needed at that pixel.  A maximum depth is not
-// negative (0 = never wet), so the corrected one is clipped at 0 when asked.
-__global__ void apply_kernel(const float *__restrict__ Y, const float *__restrict__ base, long long npix,
-                             int clip_depth, const float *__restrict__ E, float k, float *__restrict__ out_h,
-                             float *__restrict__ out_b) {
+// Corrected fields of one image's fine cells: base + scale * output channel.
+// With an envelope E, each channel's residual is first clamped to
+// +-k E[c][p], k times the largest residual the training pairs needed at
+// that cell.  A maximum depth is not negative (0 = never wet), so the
+// corrected one is clipped at 0 when asked.  out = [4][H*W]: corrected
+// maximum depth and bed change, then the interpolated ones.
+__global__ void apply_kernel(const float *__restrict__ Y, const float *__restrict__ base, Canvas cv, int clip_depth,
+                             const float *__restrict__ E, float k, float *__restrict__ out) {
+    const long long npix = (long long)cv.H * cv.W;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < npix;
          p += (long long)gridDim.x * blockDim.x) {
-        float y0 = Y[p * C], y1 = Y[p * C + 1];
+        const int y = (int)(p / cv.W), x = (int)(p - (long long)y * cv.W);
+        const long long gp = (long long)(y + kPad) * cv.Wp + (x + kPad);
+        float y0 = Y[gp * C], y1 = Y[gp * C + 1];
         if (E) {
             const float e0 = k * E[p], e1 = k * E[npix + p];
             y0 = fminf(fmaxf(y0, -e0), e0);
             y1 = fminf(fmaxf(y1, -e1), e1);
         }
-        const float hc = base[p * 2] + kSh * y0;
-        out_h[p] = clip_depth ? fmaxf(hc, 0.f) : hc;
-        out_b[p] = base[p * 2 + 1] + kSb * y1;
+        const float hb = base[gp * 2], bb = base[gp * 2 + 1];
+        const float hc = hb + kSh * y0;
+        out[p] = clip_depth ? fmaxf(hc, 0.f) : hc;
+        out[npix + p] = bb + kSb * y1;
+        out[2 * npix + p] = hb;
+        out[3 * npix + p] = bb;
     }
 }
 
@@ -988,6 +1030,7 @@ using namespace tsu::corr;
 struct TsuCorrector {
     int device = 0;
     int H = 0, W = 0, f = 1, hc = 0, wc = 0, max_batch = 0;
+    Canvas cv{};  // the padded canvas the network runs on
     static constexpr int L = 6;
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -996,11 +1039,11 @@ struct TsuCorrector {
     float *Bm = nullptr, *mB = nullptr, *vB = nullptr, *gB = nullptr;  // [L][32]
     bf16 *Wbf = nullptr, *Wt = nullptr;
     long adam_t = 0;
-    // activations [max_batch][H][W][32]: act[0] = features, act[l] = output of layer l-1
+    // activations [max_batch][Hp][Wp][32] on the padded canvas: act[0] = features, act[l] = output of layer l-1
     bf16 *act[L] = {};
     float *Yout = nullptr;
     bf16 *g0 = nullptr, *g1 = nullptr;
-    float *T = nullptr, *base = nullptr;  // [max_batch][H][W][2]
+    float *T = nullptr, *base = nullptr;  // [max_batch][Hp][Wp][2]
     int *d_idx = nullptr;
     double *d_loss = nullptr;
     // data set
@@ -1099,8 +1142,8 @@ int forward(TsuCorrector *c, int nb) {
         ConvArgs a;
         a.X = c->act[l];
         a.nimg = nb;
-        a.H = c->H;
-        a.W = c->W;
+        a.H = c->cv.Hp;
+        a.W = c->cv.Wp;
         a.Wk = c->Wbf + (size_t)l * 32 * KROWS;
         a.bias = c->Bm + l * 32;
         a.relu = (l < L - 1);
@@ -1114,8 +1157,8 @@ int forward(TsuCorrector *c, int nb) {
 
 int load_batch(TsuCorrector *c, const int *idx, int nb, bool targets) {
     CCK(cudaMemcpyAsync(c->d_idx, idx, nb * sizeof(int), cudaMemcpyHostToDevice, c->st));
-    features_kernel<<<4 * num_sms(), 256, 0, c->st>>>(c->d_idx, nb, c->coarse, targets ? c->fine : nullptr, c->Hf, c->H,
-                                                      c->W, c->hc, c->wc, c->f, c->act[0], targets ? c->T : nullptr,
+    features_kernel<<<4 * num_sms(), 256, 0, c->st>>>(c->d_idx, nb, c->coarse, targets ? c->fine : nullptr, c->Hf, c->cv,
+                                                      c->hc, c->wc, c->f, c->act[0], targets ? c->T : nullptr,
                                                       c->base);
     CCK(cudaGetLastError());
     return TSU_OK;
@@ -1131,7 +1174,7 @@ int compute_envelope(TsuCorrector *c, int n) {
         for (int b = 0; b < nb; b++) idx[b] = s0 + b;
         const int rc = load_batch(c, idx.data(), nb, true);
         if (rc) return rc;
-        envelope_kernel<<<4 * num_sms(), 256, 0, c->st>>>(c->T, nb, npix, c->E);
+        envelope_kernel<<<4 * num_sms(), 256, 0, c->st>>>(c->T, nb, c->cv, c->E);
         CCK(cudaGetLastError());
     }
     c->env_n = n;
@@ -1148,13 +1191,14 @@ extern "C" int tsu_corr_create(TsuCorrector **out, int ny, int nx, int factor, i
     c->device = device;
     c->H = ny;
     c->W = nx;
+    c->cv = canvas(ny, nx);
     c->f = factor;
     c->hc = ny / factor;
     c->wc = nx / factor;
     c->max_batch = max_batch;
     const int L = TsuCorrector::L;
     const size_t nw = (size_t)L * 32 * KROWS, nbias = (size_t)L * 32;
-    const size_t npix = (size_t)max_batch * ny * nx;
+    const size_t npix = (size_t)max_batch * c->cv.Hp * c->cv.Wp;  // padded canvas
     cudaError_t e = cudaSetDevice(device);
 #define CAL(p, bytes) \
     if (e == cudaSuccess) e = cudaMalloc((void **)&(p), (bytes))
@@ -1313,20 +1357,21 @@ extern "C" int tsu_corr_train(TsuCorrector *c, int ntrain, int iters, int batch,
         if (rc) break;
         e = cudaMemsetAsync(c->d_loss, 0, 8, c->st);
         if (e != cudaSuccess) break;
-        loss_kernel<<<4 * num_sms(), 256, 0, c->st>>>(c->Yout, c->T, npix, c->wbig, c->g0, c->d_loss);
+        loss_kernel<<<4 * num_sms(), 256, 0, c->st>>>(c->Yout, c->T, batch, c->cv, c->wbig, c->g0, c->d_loss);
         if ((e = cudaGetLastError()) != cudaSuccess) break;
         if ((e = cudaMemcpyAsync(h_loss + it, c->d_loss, 8, cudaMemcpyDeviceToHost, c->st)) != cudaSuccess) break;
         if ((e = cudaMemsetAsync(c->gW, 0, nw * 4, c->st)) != cudaSuccess) break;
         if ((e = cudaMemsetAsync(c->gB, 0, (size_t)L * 32 * 4, c->st)) != cudaSuccess) break;
         bf16 *dZ = c->g0, *dX = c->g1;
         for (int l = L - 1; l >= 0 && e == cudaSuccess; l--) {
-            e = wgrad_launch(c->act[l], dZ, batch, c->H, c->W, c->gW + (size_t)l * 32 * KROWS, c->gB + l * 32, c->st);
+            e = wgrad_launch(c->act[l], dZ, batch, c->cv.Hp, c->cv.Wp, c->gW + (size_t)l * 32 * KROWS, c->gB + l * 32,
+                             c->st);
             if (e == cudaSuccess && l > 0) {  // dZ_{l-1} = conv(dZ_l, flipped W_l), zero where act[l] <= 0
                 ConvArgs a;
                 a.X = dZ;
                 a.nimg = batch;
-                a.H = c->H;
-                a.W = c->W;
+                a.H = c->cv.Hp;
+                a.W = c->cv.Wp;
                 a.Wk = c->Wt + (size_t)l * 32 * KROWS;
                 a.bias = nullptr;
                 a.relu = 0;
@@ -1378,29 +1423,30 @@ extern "C" int tsu_corr_predict(TsuCorrector *c, int first, int n, float *out_hm
         if (r) return r;
     }
     float *d_out = nullptr;
-    CCK(cudaMalloc((void **)&d_out, 2 * np * 4));
-    std::vector<float> bb(2 * np);
+    CCK(cudaMalloc((void **)&d_out, 4 * np * 4));
     int rc = TSU_OK;
     for (int k = 0; k < n && !rc; k++) {
         const int s = first + k;
         rc = load_batch(c, &s, 1, false);
         if (!rc) rc = forward(c, 1);
         if (rc) break;
-        apply_kernel<<<2 * num_sms(), 256, 0, c->st>>>(c->Yout, c->base, (long long)np, c->clip_depth,
-                                                         clamp ? c->E : nullptr, c->envelope, d_out, d_out + np);
-        void *outs[2] = {out_hmax + k * np, out_db + k * np};
-        const void *ins[2] = {d_out, d_out + np};
+        apply_kernel<<<2 * num_sms(), 256, 0, c->st>>>(c->Yout, c->base, c->cv, c->clip_depth, clamp ? c->E : nullptr,
+                                                         c->envelope, d_out);
+        float *want[4] = {out_hmax, out_db, base_hmax, base_db};
+        void *outs[4];
+        const void *ins[4];
+        int m = 0;
+        for (int q = 0; q < 4; q++)
+            if (want[q]) {
+                outs[m] = want[q] + k * np;
+                ins[m++] = d_out + q * np;
+            }
         if (cudaGetLastError() != cudaSuccess ||
-            tsu::planes_d2h(2, outs, (size_t)c->W * 4, ins, (size_t)c->W * 4, (size_t)c->W * 4, c->H, c->st) != cudaSuccess ||
-            cudaMemcpyAsync(bb.data(), c->base, 2 * np * 4, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+            tsu::planes_d2h(m, outs, (size_t)c->W * 4, ins, (size_t)c->W * 4, (size_t)c->W * 4, c->H, c->st) != cudaSuccess ||
             cudaStreamSynchronize(c->st) != cudaSuccess) {
             snprintf(g_corr_msg, sizeof(g_corr_msg), "tsu_corr_predict: CUDA error");
             rc = TSU_ERR_CUDA;
             break;
-        }
-        for (size_t p = 0; p < np; p++) {
-            if (base_hmax) base_hmax[k * np + p] = bb[2 * p];
-            if (base_db) base_db[k * np + p] = bb[2 * p + 1];
         }
     }
     cudaFree(d_out);
@@ -1420,8 +1466,8 @@ extern "C" int tsu_corr_bench_conv(TsuCorrector *c, int nimg, int iters, double 
     ConvArgs a;
     a.X = c->act[0];
     a.nimg = nimg;
-    a.H = c->H;
-    a.W = c->W;
+    a.H = c->cv.Hp;  // the padded canvas the network runs on
+    a.W = c->cv.Wp;
     a.Wk = c->Wbf;
     a.bias = c->Bm;
     a.relu = 1;
@@ -1437,7 +1483,7 @@ extern "C" int tsu_corr_bench_conv(TsuCorrector *c, int nimg, int iters, double 
     CCK(cudaEventElapsedTime(&ms, c->e0, c->e1));
     const double per = ms / iters;
     if (ms_per_conv) *ms_per_conv = per;
-    if (tflops) *tflops = 2.0 * nimg * (double)c->H * c->W * KROWS * 32 / (per * 1e-3) / 1e12;
+    if (tflops) *tflops = 2.0 * nimg * (double)c->cv.Hp * c->cv.Wp * KROWS * 32 / (per * 1e-3) / 1e12;
     return check_kernel_flag();
 }
 
