@@ -35,6 +35,7 @@ device-timed region.
 """
 import argparse
 import ctypes as C
+import functools
 import json
 import os
 import statistics
@@ -217,7 +218,7 @@ def traffic_from_profiles(name):
         for line in open(path):
             parts = line.split()
             if len(parts) >= 4 and parts[0] == name:
-                return float(parts[1]), float(parts[2]), parts[3]
+                return float(parts[1]), float(parts[2]), parts[3], float(parts[4]) if len(parts) > 4 else None
     except OSError:
         pass
     return None
@@ -237,7 +238,38 @@ def roofline(form, n, steps, ms, tr_key=None):
         r["traffic"] = round(tr[0] * n / 2.0, 0)
         r["traffic_source"] = ("ncu dram__bytes_read+write of this workload" if tr[2] == tr_key else
                                "ncu dram__bytes of the %s capture (%.0f cells) scaled per cell" % (tr[2], tr[1]))
+        if tr[3]:
+            # the bound that does apply: warp-instruction issue, 4 per clock per SM
+            sms, mhz = sm_count_and_max_clock()
+            peak_issue = 4.0 * sms * mhz * 1e6
+            rate = n * steps / (ms / 1e3)
+            r["issue"] = {"warp_inst_per_cell_step": tr[3], "peak_warp_inst_per_s": peak_issue,
+                          "frac": round(rate * tr[3] / peak_issue, 4),
+                          "source": "ncu smsp__inst_executed of the %s capture per cell-step; peak = 4 warp "
+                                    "instructions per clock x %d SMs x %.0f MHz" % (tr[2], sms, mhz)}
     return r
+
+
+@functools.lru_cache(maxsize=None)
+def sm_count_and_max_clock():
+    """SMs and maximum SM clock (MHz) of the current device (148, 1965 without one)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            prop = torch.cuda.get_device_properties(torch.cuda.current_device())
+            sms = prop.multi_processor_count
+        else:
+            sms = 148
+    except Exception:
+        sms = 148
+    mhz = 1965.0
+    try:
+        out = subprocess.run(["nvidia-smi", "--query-gpu=clocks.max.sm", "--format=csv,noheader,nounits", "-i",
+                              str(torch.cuda.current_device())], capture_output=True, text=True, timeout=20)
+        mhz = float(out.stdout.strip().splitlines()[0])
+    except Exception:
+        pass
+    return sms, mhz
 
 
 def form_switches(w, precision):
