@@ -39,6 +39,7 @@ struct Phys32 {
     int npx, npy;
     int order, wbc, bedload, suspension, read_files, bedload_law;
     float grass_ag;
+    int dry_skip;  // as Phys64::dry_skip (edge32)
 };
 
 // x is neither NaN nor an infinity (exponent field not all ones)
@@ -134,6 +135,12 @@ __device__ __forceinline__ float bedload32(const Phys32 &P, float h, float ux, f
 // Dp (into b) in the normal frame (components h, qn, qt, H, hc).
 __device__ __forceinline__ void edge32(const Phys32 &P, const Face32 &a, float u0, float v0, const Face32 &b,
                                        float u1, float v1, int fixed, float Dm[5], float Dp[5]) {
+    // both faces dry: zero fluctuations (the FP64 edge_flux gives the reason)
+    if (P.dry_skip && a.h == 0.f && b.h == 0.f) {
+#pragma unroll
+        for (int i = 0; i < 5; i++) Dm[i] = Dp[i] = 0.f;
+        return;
+    }
     const float c0 = a.c, c1 = b.c;
     // hydrostatic reconstruction h* = max(eta + min(H_a, H_b), 0), eta = z + eta0:
     // on an edge that is wet by a clear margin on both sides the depths are

@@ -37,6 +37,9 @@ struct Phys64 {
     // state and mask planes and filled by the halo exchange.  A whole grid
     // has ny_glob = npy, j0 = 0, gs = gn = 0.
     int ny_glob, j0, gs, gn;
+    // 1: an edge whose two faces are both dry returns zero fluctuations
+    // without evaluating the Riemann solver (see edge_flux)
+    int dry_skip;
 };
 
 // IEEE quotient and square root with the zero cases answered directly:
@@ -158,6 +161,18 @@ __device__ __forceinline__ void phys_flux(const Phys64 &P, double h, double ux, 
 // fluctuation into side a, Dp into side b, both in x/y components.
 __device__ __forceinline__ void edge_flux(const Phys64 &P, const State5 &a, const State5 &b, int nx, int ny,
                                           int fixed, double Dm[5], double Dp[5]) {
+    // Both faces dry (h == 0 exactly, which also excludes NaN): every
+    // velocity, flux and depth below is a zero, the hydrostatic depths are
+    // max(-H + min(H_a, H_b), 0) = 0, both wave speeds are 0, so a0 = a1 = 0
+    // and all ten fluctuations evaluate to zeros.  They are returned as +0
+    // (the full evaluation can give -0 for some; a zero's sign does not
+    // reach any non-zero value of this scheme).  Dry land makes this the
+    // common edge of a coastal grid.
+    if (P.dry_skip && a.h == 0.0 && b.h == 0.0) {
+#pragma unroll
+        for (int i = 0; i < 5; i++) Dm[i] = Dp[i] = 0.0;
+        return;
+    }
     const double dnx = (double)nx, dny = (double)ny;
     double qlx = a.qx * dnx + a.qy * dny;
     double qly = a.qy * dnx - a.qx * dny;

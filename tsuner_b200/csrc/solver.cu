@@ -152,6 +152,13 @@ static void free_all(TsuSolver *s) {
     if (s->own_st) cudaStreamDestroy(s->own_st);
 }
 
+// TSU_DRY_SKIP=0 evaluates the Riemann solver on dry-dry edges too (for
+// measurement; the results are the same values)
+static int dry_skip_enabled() {
+    const char *e = std::getenv("TSU_DRY_SKIP");
+    return (e && e[0] == '0') ? 0 : 1;
+}
+
 static void fill_phys(TsuSolver *s) {
     const SimParams *p = &s->p;
     const TsuSwitches *sw = &s->sw;
@@ -184,6 +191,7 @@ static void fill_phys(TsuSolver *s) {
     P.j0 = s->j0;
     P.gs = s->gs;
     P.gn = s->gn;
+    P.dry_skip = dry_skip_enabled();
     Phys32 &Q = s->phys32;
     Q.eta0 = sw->eta0;
     Q.eta0f = (float)sw->eta0;
@@ -216,6 +224,7 @@ static void fill_phys(TsuSolver *s) {
     Q.read_files = sw->read_files;
     Q.bedload_law = sw->bedload_law;
     Q.grass_ag = (float)sw->grass_ag;
+    Q.dry_skip = dry_skip_enabled();
 }
 
 // A solver for global rows [j0, j1) of the grid p (the whole grid: 0, npy),
