@@ -78,6 +78,16 @@ __device__ __forceinline__ void recon32(const Phys32 &P, const float *s, int c, 
     const float hi = s[5 * PS + c], hl = s[5 * PS + l], hr = s[5 * PS + r];
     const float zi = s[c], zl = s[l], zr = s[r];
     const float Hi = s[PS + c], Hl = s[PS + l], Hr = s[PS + r];
+    if (P.dry_skip && hi == 0.f && hl == 0.f && hr == 0.f) {
+        // a dry stencil: every slope is 0, both faces are dry faces of bed
+        // H_i (what filter32 makes of them) and deta = 0
+        fm.h = fm.u = fm.v = fm.c = 0.f;
+        fm.H = Hi;
+        fm.z = dry_z(Hi, P.eta0);
+        fp = fm;
+        deta = 0.f;
+        return;
+    }
     float dh = limiter32(hi - hl, hr - hi);
     if (0.5f * fabsf(dh) > hi) dh = copysignf(2.f * hi, dh);
     // hydrostatic eta slope (GPU/Reconstructor.cu:157-162): differences of

@@ -380,9 +380,19 @@ __global__ void __launch_bounds__(NTHR, MINB) stage64_kernel(const __grid_consta
         State5 fm, fp;
         if (ORDER == 2) {
             double deta;
-            reconstruct_dir<PS>(sV, sUC, c, c - step, c + step, fm, fp, deta);
-            filter5(fm);  // GPU/Reconstructor.cu:344-348
-            filter5(fp);
+            if (P.dry_skip && sV[c] == 0.0 && sV[c - step] == 0.0 && sV[c + step] == 0.0) {
+                // a dry stencil: every slope is avg(0, 0) = 0, so both faces
+                // are (0, q_i, 0, H_i, 0 * c) before the filter and (0, 0, 0,
+                // H_i, 0) after it (zeros up to their sign), and deta = 0
+                fm.h = fm.qx = fm.qy = fm.hc = 0.0;
+                fm.H = sV[3 * PS + c];
+                fp = fm;
+                deta = 0.0;
+            } else {
+                reconstruct_dir<PS>(sV, sUC, c, c - step, c + step, fm, fp, deta);
+                filter5(fm);  // GPU/Reconstructor.cu:344-348
+                filter5(fp);
+            }
             if (didx >= 0) sDeta[didx] = deta;
         } else {  // first order: faces are the cell values (GPU/Reconstructor.cu:99-107)
             fm = get5(sV + c, PS);
