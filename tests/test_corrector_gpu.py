@@ -317,3 +317,23 @@ def test_both_forward_kernels_give_identical_outputs(tmp_path):
         out[name] = np.load(path)
     assert np.abs(out["ws"]).max() > 0
     assert np.array_equal(out["ws"], out["plain"])
+
+
+def test_training_is_reproducible():
+    """The weight gradient adds its per-CTA partials in a fixed order, so two
+    trainings from the same seed on the same samples give the same weights
+    bit for bit (the loss sums may differ in their last bits)."""
+    dev()
+    ny, f = 64, 4
+    Hf, coarse, fine = synthetic_samples(8, ny, f, 9)
+    out = []
+    for _ in range(2):
+        c = K.Corrector(ny, ny, f, max_batch=4, seed=3)
+        try:
+            c.set_site(Hf)
+            c.add_samples(coarse, fine)
+            c.train(ntrain=8, iters=30, batch=4, lr=2e-3, seed=5)
+            out.append(c.weights())
+        finally:
+            c.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])

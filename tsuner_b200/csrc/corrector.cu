@@ -560,10 +560,14 @@ __global__ void __launch_bounds__(kWsThreads) conv3x3_fwd_ws_kernel(ConvArgs a, 
     if (warp == 1) tmem_dealloc(tmem, 32 * kWsAcc);
 }
 
-// Weight (and bias) gradient, accumulated into dW[cout][288] and db[32].
+// Weight (and bias) gradient partials of this CTA's strip of tiles, written
+// to its row of `part` ([gridDim.x][kWgPart]: dW[cout][288], then the 4 warps'
+// bias sums [4][32]); wgrad_reduce_kernel adds the rows to dW and db in a
+// fixed order, so the gradient does not depend on which CTA finishes first.
+constexpr int kWgPart = 32 * KROWS + 4 * 32;
 __global__ void __launch_bounds__(128, kWgCtasPerSm)
     conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmXr, const __grid_constant__ CUtensorMap tmZ, int nimg,
-                         int H, int W, float *__restrict__ dW, float *__restrict__ db) {
+                         int H, int W, float *__restrict__ part) {
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = smem_align<1024>(sm_raw);  // two stages: patch (12288 B) + dZ planes (4 x 2048 B)
     uint64_t *full = reinterpret_cast<uint64_t *>(sm + 2 * kWgStage);  // [2] stage loaded
@@ -665,6 +669,9 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
         __syncthreads();
     }
     const int n = i;  // iterations entered (the last may have failed)
+    float *prow = part + (size_t)blockIdx.x * kWgPart;
+    if (failed || n == 0)  // no partials from this CTA
+        for (int k = tid; k < kWgPart; k += 128) prow[k] = 0.f;
     if (failed) {
         if (tid == 0) {
             atomicExch(&g_corr_err, 1);
@@ -678,6 +685,7 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
         const int L = n - 1;
         const bool ok = mbar_wait_first(&done[L & 1], (L >> 1) & 1);
         if (__syncthreads_or(!ok)) {
+            for (int k = tid; k < kWgPart; k += 128) prow[k] = 0.f;
             if (tid == 0) {
                 atomicExch(&g_corr_err, 1);
                 mbar_wait(&done[L & 1], (L >> 1) & 1);  // the MMAs before TMEM is freed
@@ -691,24 +699,23 @@ __global__ void __launch_bounds__(128, kWgCtasPerSm)
                     tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(dx * 32), v);
                     const int m = (warp * 3 + dx) * 32 + lane;  // tap * 32 + cin
 #pragma unroll
-                    for (int c = 0; c < 32; c++) atomicAdd(dW + c * KROWS + m, v[c]);
+                    for (int c = 0; c < 32; c++) prow[c * KROWS + m] = v[c];
                 }
             }
-            if (db) {
 #pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    float v = dbp[k];
-                    v += __shfl_xor_sync(0xffffffffu, v, 4);
-                    v += __shfl_xor_sync(0xffffffffu, v, 8);
-                    v += __shfl_xor_sync(0xffffffffu, v, 16);
-                    dbp[k] = v;
-                }
-                if (lane < 4) {
+            for (int k = 0; k < 8; k++) {
+                float v = dbp[k];
+                v += __shfl_xor_sync(0xffffffffu, v, 4);
+                v += __shfl_xor_sync(0xffffffffu, v, 8);
+                v += __shfl_xor_sync(0xffffffffu, v, 16);
+                dbp[k] = v;
+            }
+            if (lane < 4) {
+                float *pb = prow + 32 * KROWS + warp * 32;
 #pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        atomicAdd(db + q * 8 + 2 * lane, dbp[2 * q]);
-                        atomicAdd(db + q * 8 + 2 * lane + 1, dbp[2 * q + 1]);
-                    }
+                for (int q = 0; q < 4; q++) {
+                    pb[q * 8 + 2 * lane] = dbp[2 * q];
+                    pb[q * 8 + 2 * lane + 1] = dbp[2 * q + 1];
                 }
             }
         }
@@ -1001,7 +1008,31 @@ cudaError_t make_map_rowq(CUtensorMap *m, const void *base, int nimg, int H, int
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-cudaError_t wgrad_launch(const bf16 *X, const bf16 *dZ, int nimg, int H, int W, float *dW, float *db, cudaStream_t st) {
+// dW[k] += sum over CTAs b (in order) of part[b][k]; db[n] += sum over b and
+// the 4 warps (in order) of the bias partials
+__global__ void wgrad_reduce_kernel(const float *__restrict__ part, int nctas, float *__restrict__ dW,
+                                    float *__restrict__ db) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < 32 * KROWS) {
+        float acc = 0.f;
+        for (int b = 0; b < nctas; b++) acc += part[(size_t)b * kWgPart + k];
+        dW[k] += acc;
+    } else if (db && k < 32 * KROWS + 32) {
+        const int n = k - 32 * KROWS;
+        float acc = 0.f;
+        for (int b = 0; b < nctas; b++)
+            for (int w = 0; w < 4; w++) acc += part[(size_t)b * kWgPart + 32 * KROWS + w * 32 + n];
+        db[n] += acc;
+    }
+}
+
+// CTAs of a weight-gradient launch (4 persistent CTAs per SM: 128 TMEM columns each)
+int wgrad_ctas(int nimg, int H, int W) { return std::min(tile_geom(nimg, H, W).total, kWgCtasPerSm * num_sms()); }
+
+// part: wgrad_ctas(...) * kWgPart floats of device scratch, or null (then
+// allocated on the stream for this call)
+cudaError_t wgrad_launch(const bf16 *X, const bf16 *dZ, int nimg, int H, int W, float *dW, float *db, float *part,
+                         cudaStream_t st) {
     cudaError_t e = prepare();
     if (e != cudaSuccess) return e;
     if (reinterpret_cast<uintptr_t>(X) % 16 || reinterpret_cast<uintptr_t>(dZ) % 16) return cudaErrorInvalidValue;
@@ -1009,11 +1040,24 @@ cudaError_t wgrad_launch(const bf16 *X, const bf16 *dZ, int nimg, int H, int W, 
     e = make_map_rowq(&mx, X, nimg, H, W);
     if (e == cudaSuccess) e = make_map(&mz, dZ, nimg, H, W, TXP, TYP);
     if (e != cudaSuccess) return e;
-    const TileGeom G = tile_geom(nimg, H, W);
-    // 4 persistent CTAs per SM: 128 TMEM columns each
-    const int ctas = std::min(G.total, kWgCtasPerSm * num_sms());
-    conv3x3_wgrad_kernel<<<ctas, 128, kWgSmem, st>>>(mx, mz, nimg, H, W, dW, db);
-    return cudaGetLastError();
+    const int ctas = wgrad_ctas(nimg, H, W);
+    float *own = nullptr;
+    if (!part) {
+        e = cudaMallocAsync((void **)&own, (size_t)ctas * kWgPart * sizeof(float), st);
+        if (e != cudaSuccess) return e;
+        part = own;
+    }
+    conv3x3_wgrad_kernel<<<ctas, 128, kWgSmem, st>>>(mx, mz, nimg, H, W, part);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        wgrad_reduce_kernel<<<(32 * KROWS + 32 + 255) / 256, 256, 0, st>>>(part, ctas, dW, db);
+        e = cudaGetLastError();
+    }
+    if (own) {
+        const cudaError_t f = cudaFreeAsync(own, st);
+        if (e == cudaSuccess) e = f;
+    }
+    return e;
 }
 
 }  // namespace corr
@@ -1060,6 +1104,7 @@ struct TsuCorrector {
     // [0, env_n) ([2][H*W]); ntrain = the training set of the last tsu_corr_train
     float *E = nullptr;
     int env_n = 0, ntrain = 0;
+    float *wg_part = nullptr;  // weight-gradient partials of one layer ([CTAs][kWgPart])
 };
 
 namespace {
@@ -1083,7 +1128,7 @@ double uniform01(uint64_t &s) { return (double)(splitmix(s) >> 11) * (1.0 / 9007
 
 void free_all(TsuCorrector *c) {
     float *fp[] = {c->Wm, c->mW, c->vW, c->gW, c->Bm, c->mB, c->vB, c->gB, c->Yout, c->T, c->base, c->Hf, c->coarse, c->fine,
-                   c->E};
+                   c->E, c->wg_part};
     for (float *p : fp) cudaFree(p);
     cudaFree(c->Wbf);
     cudaFree(c->Wt);
@@ -1225,6 +1270,7 @@ extern "C" int tsu_corr_create(TsuCorrector **out, int ny, int nx, int factor, i
     CAL(c->d_loss, 8);
     CAL(c->Hf, (size_t)ny * nx * 4);
     CAL(c->E, (size_t)2 * ny * nx * 4);
+    CAL(c->wg_part, (size_t)wgrad_ctas(max_batch, c->cv.Hp, c->cv.Wp) * kWgPart * 4);
 #undef CAL
     if (e == cudaSuccess) e = prepare();
     if (e != cudaSuccess) {
@@ -1365,7 +1411,7 @@ extern "C" int tsu_corr_train(TsuCorrector *c, int ntrain, int iters, int batch,
         bf16 *dZ = c->g0, *dX = c->g1;
         for (int l = L - 1; l >= 0 && e == cudaSuccess; l--) {
             e = wgrad_launch(c->act[l], dZ, batch, c->cv.Hp, c->cv.Wp, c->gW + (size_t)l * 32 * KROWS, c->gB + l * 32,
-                             c->st);
+                             c->wg_part, c->st);
             if (e == cudaSuccess && l > 0) {  // dZ_{l-1} = conv(dZ_l, flipped W_l), zero where act[l] <= 0
                 ConvArgs a;
                 a.X = dZ;
@@ -1516,7 +1562,7 @@ extern "C" int tsu_corr_conv3x3(const void *X, int nimg, int H, int W, const voi
 extern "C" int tsu_corr_conv3x3_wgrad(const void *X, const void *dZ, int nimg, int H, int W, float *dW, float *db,
                                       void *stream) {
     if (!X || !dZ || !dW || nimg < 1 || H < 1 || W < 1) return TSU_ERR_INVALID;
-    CCK(wgrad_launch(static_cast<const bf16 *>(X), static_cast<const bf16 *>(dZ), nimg, H, W, dW, db,
+    CCK(wgrad_launch(static_cast<const bf16 *>(X), static_cast<const bf16 *>(dZ), nimg, H, W, dW, db, nullptr,
                      static_cast<cudaStream_t>(stream)));
     return TSU_OK;
 }
