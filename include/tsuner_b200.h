@@ -218,7 +218,9 @@ int tsu_get_time(TsuSolver *s, double *t, double *dt, long *steps);
  * h (water volume / cell area) and of H + hc (bed + suspended sediment). */
 int tsu_get_sums(TsuSolver *s, double *water, double *sediment);
 int tsu_get_consts(TsuSolver *s, TsuConsts *k);
-/* Device timing of the last tsu_step() call in ms (CUDA events). */
+/* Device timing of the last tsu_step() call in ms (CUDA events around its
+ * kernels; the one-time CUDA-graph build of the first call of 16 or more
+ * steps happens before them). */
 int tsu_last_step_ms(TsuSolver *s, double *ms);
 /* Number of kernel launches the last tsu_step() issued. */
 int tsu_last_step_launches(TsuSolver *s, long *launches);

