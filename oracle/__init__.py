@@ -263,12 +263,19 @@ def ref_switches(variant="default"):
     return dict(zip(("order", "rk", "wbc", "bedload", "suspension", "read_files"), out.tolist()))
 
 
-def ref_run(variant, p, V, mask=None, CC=None, tCC=None, nsteps=1, device=0):
-    """Runs the reference build for nsteps; returns dict with V, extrema, t, dt, ms."""
+def ref_run(variant, p, V, mask=None, CC=None, tCC=None, nsteps=1, device=0, work=None, ext=None):
+    """Runs the reference build for nsteps; returns dict with V, extrema, t, dt, ms.
+    work: optional float64 buffer of 5*npx*npy elements that holds the state
+    on entry and receives it on return (used in place, e.g. pinned memory);
+    ext: optional three buffers of npx*npy doubles for the extrema."""
     n = p.npx * p.npy
-    Vh = np.ascontiguousarray(V, np.float64).reshape(-1).copy()
+    if work is None:
+        Vh = np.ascontiguousarray(V, np.float64).reshape(-1).copy()
+    else:
+        Vh = work.reshape(-1)
+        assert Vh.dtype == np.float64 and Vh.size == 5 * n and Vh.flags.c_contiguous
     m = np.ones(n, np.int32) if mask is None else np.ascontiguousarray(mask, np.int32).reshape(-1)
-    hmax, bmin, eta = np.empty(n), np.empty(n), np.empty(n)
+    hmax, bmin, eta = (np.empty(n), np.empty(n), np.empty(n)) if ext is None else (e.reshape(-1) for e in ext)
     t, dt, ms = C.c_double(), C.c_double(), C.c_double()
     steps = C.c_long()
     CCa = None if CC is None else np.ascontiguousarray(CC, np.float64)
