@@ -206,7 +206,8 @@ struct ConvArgs {
     int relu;            // apply max(., 0)
     const bf16 *gate;    // optional: zero output channel n where gate[p][n] <= 0
     bf16 *Ybf;           // BF16 output, or
-    float *Yf;           // FP32 output
+    float *Yf;           // FP32 output, or
+    float *Y2;           // FP32 output of channels 0 and 1 only, [pixel][2] (the corrector's last layer)
 };
 
 // Epilogue of one tile: TMEM accumulators (lane = pixel, column = output
@@ -266,6 +267,10 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs &a, const TileGeom 
     uint4 *sw = reinterpret_cast<uint4 *>(stage + warp * 2048);
     const int rx = lane >> 2, kc = lane & 3;  // row phase: pixel in the tile row, 16-byte chunk
     const int own = (lane >> 1) & 3;          // swizzle of this lane's own pixel
+    if (a.Y2) {  // the two used channels: 8 B per pixel, a tile row is 64 contiguous bytes
+        if (inside) *reinterpret_cast<float2 *>(a.Y2 + (o / C) * 2) = make_float2(acc[0], acc[1]);
+        return;
+    }
     if (a.Yf) {  // FP32: two halves of 16 channels (64 B per pixel) through the same 2 KB
 #pragma unroll
         for (int hf = 0; hf < 2; hf++) {
@@ -829,8 +834,8 @@ __global__ void loss_kernel(const float *__restrict__ Y, const float *__restrict
         if (unpad(cv, xp, yp, x, y)) {
             const float t0 = T[g * 2];
             w0 = 1.f + wbig * t0 * t0;
-            d0 = Y[g * C] - t0;
-            d1 = Y[g * C + 1] - T[g * 2 + 1];
+            d0 = Y[g * 2] - t0;
+            d1 = Y[g * 2 + 1] - T[g * 2 + 1];
             acc += (double)w0 * d0 * d0 + (double)d1 * d1;
         }
         uint4 *gp = reinterpret_cast<uint4 *>(dY + g * C);
@@ -908,7 +913,7 @@ __global__ void apply_kernel(const float *__restrict__ Y, const float *__restric
          p += (long long)gridDim.x * blockDim.x) {
         const int y = (int)(p / cv.W), x = (int)(p - (long long)y * cv.W);
         const long long gp = (long long)(y + kPad) * cv.Wp + (x + kPad);
-        float y0 = Y[gp * C], y1 = Y[gp * C + 1];
+        float y0 = Y[gp * 2], y1 = Y[gp * 2 + 1];
         if (E) {
             const float e0 = k * E[p], e1 = k * E[npix + p];
             y0 = fminf(fmaxf(y0, -e0), e0);
@@ -1085,7 +1090,7 @@ struct TsuCorrector {
     long adam_t = 0;
     // activations [max_batch][Hp][Wp][32] on the padded canvas: act[0] = features, act[l] = output of layer l-1
     bf16 *act[L] = {};
-    float *Yout = nullptr;
+    float *Yout = nullptr;  // the last layer's output channels 0 and 1 [max_batch][Hp][Wp][2]
     bf16 *g0 = nullptr, *g1 = nullptr;
     float *T = nullptr, *base = nullptr;  // [max_batch][Hp][Wp][2]
     int *d_idx = nullptr;
@@ -1180,7 +1185,8 @@ int check_kernel_flag() {
     return TSU_OK;
 }
 
-// forward pass of `nb` images already in act[0]; FP32 output in Yout
+// forward pass of `nb` images already in act[0]; the last layer's two used
+// output channels in Yout ([pixel][2], FP32)
 int forward(TsuCorrector *c, int nb) {
     const int L = TsuCorrector::L;
     for (int l = 0; l < L; l++) {
@@ -1194,7 +1200,8 @@ int forward(TsuCorrector *c, int nb) {
         a.relu = (l < L - 1);
         a.gate = nullptr;
         a.Ybf = (l < L - 1) ? c->act[l + 1] : nullptr;
-        a.Yf = (l < L - 1) ? nullptr : c->Yout;
+        a.Yf = nullptr;
+        a.Y2 = (l < L - 1) ? nullptr : c->Yout;
         CCK(conv_launch(a, c->st));
     }
     return TSU_OK;
@@ -1261,7 +1268,7 @@ extern "C" int tsu_corr_create(TsuCorrector **out, int ny, int nx, int factor, i
     CAL(c->Wbf, nw * 2);
     CAL(c->Wt, nw * 2);
     for (int l = 0; l < L; l++) CAL(c->act[l], npix * C * 2);
-    CAL(c->Yout, npix * C * 4);
+    CAL(c->Yout, npix * 2 * 4);
     CAL(c->g0, npix * C * 2);
     CAL(c->g1, npix * C * 2);
     CAL(c->T, npix * 2 * 4);
@@ -1424,6 +1431,7 @@ extern "C" int tsu_corr_train(TsuCorrector *c, int ntrain, int iters, int batch,
                 a.gate = c->act[l];
                 a.Ybf = dX;
                 a.Yf = nullptr;
+                a.Y2 = nullptr;
                 e = conv_launch(a, c->st);
                 std::swap(dZ, dX);
             }
@@ -1520,6 +1528,7 @@ extern "C" int tsu_corr_bench_conv(TsuCorrector *c, int nimg, int iters, double 
     a.gate = nullptr;
     a.Ybf = c->act[1];
     a.Yf = nullptr;
+    a.Y2 = nullptr;
     for (int k = 0; k < 3; k++) CCK(conv_launch(a, c->st));
     CCK(cudaEventRecord(c->e0, c->st));
     for (int k = 0; k < iters; k++) CCK(conv_launch(a, c->st));
@@ -1555,6 +1564,7 @@ extern "C" int tsu_corr_conv3x3(const void *X, int nimg, int H, int W, const voi
     a.gate = static_cast<const bf16 *>(gate);
     a.Ybf = static_cast<bf16 *>(Ybf);
     a.Yf = Yf;
+    a.Y2 = nullptr;
     CCK(conv_launch(a, static_cast<cudaStream_t>(stream)));
     return TSU_OK;
 }
