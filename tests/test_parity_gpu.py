@@ -285,9 +285,39 @@ def test_config2_full_5000_steps_vs_reference_build():
     ("rk0_order1", dict(order=1, wbc=1, read_files=1, rk=0)),
 ])
 def test_switch_variants_vs_reference_build(variant, sw):
-    w = W.nwave_shelf(72, 56, 40.0, slr=0.5, amp=2.0, period=300.0, t_series=300.0)
+    # without the boundary series the shelf would stay at rest: those
+    # variants run a collapsing hump over a bed with non-erodible blocks
+    if sw["read_files"]:
+        w = W.nwave_shelf(72, 56, 40.0, slr=0.5, amp=2.0, period=300.0, t_series=300.0)
+    else:
+        w = W.hump(72, 56, 10.0, sigma=120.0)
+        w.mask = W.harbour_mask(72, 56, np.random.default_rng(3))
     w.sw = make_switches(**sw)
     ref_vs_new(w, 150, variant, w.sw)
+
+
+@need_ref
+@pytest.mark.parametrize("variant,sw,steps", [
+    ("rk0", dict(order=2, wbc=1, read_files=1, rk=0), 400),
+    ("rf0_wbc2", dict(order=2, wbc=2, read_files=0), 400),
+], ids=["muscl_hancock", "periodic"])
+def test_switch_variants_at_1024x768_vs_reference_build(variant, sw, steps):
+    """Two switch paths on 0.8 M cells for 400 steps: MUSCL-Hancock on the
+    shelf (the N-wave series, the harbour mask, ~20 % dry land), the periodic
+    boundaries on a collapsing hump with non-erodible blocks (without the
+    series the shelf would stay at rest, and its momentum would be round-off
+    only).  Value for value against the -nolto build of that variant, within
+    1e-12 of its recipe build."""
+    if sw["read_files"]:
+        w = W.nwave_shelf(1024, 768, 10.0, slr=0.5, amp=3.0, period=300.0, t_series=400.0)
+    else:
+        w = W.hump(1024, 768, 2.5, sigma=300.0)  # 2.56 km: the 2 % slope stays under water
+        w.mask = W.harbour_mask(1024, 768, np.random.default_rng(4))
+    w.sw = make_switches(**sw)
+    new, ref = ref_vs_new(w, steps, variant, w.sw)
+    errs = {name: rel_err(new["V"][f], ref["V"][f]) for f, name in enumerate(FIELDS)}
+    print("%s vs the recipe build after %d steps: " % (variant, steps) +
+          ", ".join("%s %.2e" % kv for kv in errs.items()))
 
 
 def test_manning_vs_reference_build():

@@ -27,7 +27,18 @@ def cases():
         "free_2": (hump, make_switches(order=2, wbc=0, read_files=0), 2, 60),
         "periodic_2": (hump, make_switches(order=2, wbc=2, read_files=0), 2, 60),
         "periodic_series_3": (small, make_switches(order=2, wbc=2, read_files=1), 3, 60),
+        # a grid of 2 M cells in 8 slabs (the split of an 8-GPU node), the shelf workload
+        "shelf_2048x1024_8_slabs": (big(), big().sw, 8, 40),
     }
+
+
+_BIG = []
+
+
+def big():
+    if not _BIG:
+        _BIG.append(W.nwave_shelf(2048, 1024, 10.0, slr=0.5, amp=3.0, period=300.0, t_series=300.0))
+    return _BIG[0]
 
 
 @pytest.mark.parametrize("name", sorted(cases()))
