@@ -249,7 +249,7 @@ def test_set_weights_round_trip_and_conv_bench():
 
 def test_held_out_sources_improve_on_interpolation():
     """The whole pipeline at a small size: pairs from FP32 ensembles on a 128^2
-    site (coarse 32^2), held-out sources judged against the FP64 plain fine
+    site (coarse 32^2), held-out sources compared with the FP64 plain fine
     solve.  With the options the bench uses (large-residual weight 16, depth
     clip, envelope 1) the corrector's maximum-depth and bed-change RMSE are
     below those of the interpolation alone, and its maximum-depth L-inf is
